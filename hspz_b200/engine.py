@@ -1,0 +1,191 @@
+"""Python view of the B200 engine, shaped like the reference's ``Engine``
+(src/gpu/mod.rs:817-2307) and its pass driver ``seed_and_filter_all``
+(src/run.rs:266-495).  All work happens in libhspz_b200.so through the C ABI;
+this module only marshals host buffers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import _native as N
+from .hsp import PASS_RECORD, SEGMENT_PAIR
+from .scoring import build_sub_mat
+from .sequence import as_bytes
+
+BATCH_RECORD = np.dtype([("query", "<u4"), ("interval", "<u4"), ("strand", "<u4"), ("_pad", "<u4"),
+                         ("ref_start", "<u4"), ("query_start", "<u4"), ("len", "<u4"), ("score", "<i4")])
+
+
+@dataclass
+class EngineConfig:
+    """Run flags that parameterise the path (src/cli.rs:41-183) and the
+    EngineConfig knobs (src/gpu/mod.rs:1005-1019)."""
+    sub_mat: List[int] = field(default_factory=lambda: build_sub_mat("", 910))
+    seed: str = "12of19"
+    xdrop: int = 910
+    hspthresh: int = 3000
+    noentropy: bool = False
+    transitions: bool = True
+    step: int = 1
+    max_hits: int = 16711680
+    occ_cap: int = 0
+    wga_chunk: int = 250_000
+    interval: int = 10_000_000
+    strand: str = "both"
+
+    def to_c(self) -> N.ConfigC:
+        c = N.ConfigC()
+        if len(self.sub_mat) != 64:
+            raise ValueError("sub_mat must have 64 entries")
+        for i, v in enumerate(self.sub_mat):
+            c.sub_mat[i] = int(v)
+        c.seed = self.seed.encode()[:63]
+        c.xdrop, c.hspthresh = int(self.xdrop), int(self.hspthresh)
+        c.noentropy, c.transitions = int(bool(self.noentropy)), int(bool(self.transitions))
+        c.step, c.max_hits, c.occ_cap = int(self.step), int(self.max_hits), int(self.occ_cap)
+        c.wga_chunk, c.interval = int(self.wga_chunk), int(self.interval)
+        strands = {"plus": 1, "minus": 2, "both": 3}
+        if self.strand not in strands:
+            raise ValueError(f"--strand must be plus, minus or both, got {self.strand}")
+        c.strand = strands[self.strand]
+        return c
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _take(ptr: C.c_void_p, n: int, dtype) -> np.ndarray:
+    if not ptr.value or n == 0:
+        if ptr.value:
+            N.lib().hz_free(ptr)
+        return np.zeros(0, dtype=dtype)
+    raw = (C.c_uint8 * (n * dtype.itemsize)).from_address(ptr.value)
+    arr = np.frombuffer(raw, dtype=dtype).copy()
+    N.lib().hz_free(ptr)
+    return arr
+
+
+def shape_info(seed: str = "12of19"):
+    """(width, care positions) of a seed pattern (Shape::parse, src/seed.rs:49-79)."""
+    size, k = C.c_uint32(), C.c_uint32()
+    N.check(N.lib().hz_shape_info(seed.encode(), C.byref(size), C.byref(k)))
+    return size.value, k.value
+
+
+class Engine:
+    """One engine per device; owns the resident target and the query."""
+
+    def __init__(self, config: Optional[EngineConfig] = None, device: int = 0):
+        self.config = config or EngineConfig()
+        self._h = C.c_void_p()
+        N.check(N.lib().hz_engine_create(C.byref(self.config.to_c()), device, C.byref(self._h)))
+        self.seed_size, self.kmer_size = shape_info(self.config.seed)
+
+    def close(self):
+        if self._h and self._h.value:
+            N.lib().hz_engine_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- target -----------------------------------------------------------
+    def load_tables(self, index_table: np.ndarray, pos_table: np.ndarray, ref_seq: np.ndarray):
+        """Engine::new's host-built tables (src/gpu/mod.rs:1005-1041)."""
+        it = np.ascontiguousarray(index_table, dtype=np.uint32)
+        pt = np.ascontiguousarray(pos_table, dtype=np.uint32)
+        rs = np.ascontiguousarray(ref_seq, dtype=np.uint8)
+        N.check(N.lib().hz_engine_load_tables(self._h, _ptr(it), it.size, _ptr(pt), pt.size, _ptr(rs), rs.size))
+
+    def load_target(self, ref_ascii):
+        """Build the seed table on the device from the ASCII reference block."""
+        a = np.ascontiguousarray(as_bytes(ref_ascii))
+        N.check(N.lib().hz_engine_load_target(self._h, _ptr(a), a.size))
+
+    def read_tables(self):
+        il, pl = C.c_uint64(), C.c_uint64()
+        N.check(N.lib().hz_engine_read_tables(self._h, None, C.byref(il), None, C.byref(pl)))
+        it = np.zeros(il.value, dtype=np.uint32)
+        pt = np.zeros(max(pl.value, 1), dtype=np.uint32)
+        N.check(N.lib().hz_engine_read_tables(self._h, _ptr(it), C.byref(il), _ptr(pt), C.byref(pl)))
+        return it, pt[: pl.value]
+
+    # --- query ------------------------------------------------------------
+    def swap_query(self, query: np.ndarray, query_rc: np.ndarray):
+        """Engine::swap_query with both strands in the device alphabet."""
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        r = np.ascontiguousarray(query_rc, dtype=np.uint8)
+        if q.size != r.size:
+            raise ValueError("query and query_rc differ in length")
+        N.check(N.lib().hz_swap_query(self._h, _ptr(q), _ptr(r), q.size))
+
+    def swap_query_ascii(self, query_ascii):
+        a = np.ascontiguousarray(as_bytes(query_ascii))
+        N.check(N.lib().hz_swap_query_ascii(self._h, _ptr(a), a.size))
+
+    # --- per call -----------------------------------------------------------
+    def upload_seeds(self, slot: int, seeds: np.ndarray):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        N.check(N.lib().hz_upload_seeds(self._h, slot, _ptr(s), s.size))
+
+    def generate_seeds(self, slot: int, rev: bool, rng, transitions: Optional[bool] = None) -> int:
+        t = self.config.transitions if transitions is None else transitions
+        n = C.c_uint64()
+        N.check(N.lib().hz_generate_seeds(self._h, slot, int(bool(rev)), int(rng[0]), int(rng[1]), int(bool(t)),
+                                          C.byref(n)))
+        return n.value
+
+    def seed_and_filter(self, slot: int, rev: bool):
+        """FilterOutput: (hsps deduped per MAX_HITS chunk in LASTZ order, stats)."""
+        out, n, st = C.c_void_p(), C.c_uint64(), N.StatsC()
+        N.check(N.lib().hz_seed_and_filter(self._h, slot, int(bool(rev)), C.byref(out), C.byref(n), C.byref(st)))
+        return _take(out, n.value, SEGMENT_PAIR), st.as_dict()
+
+    def run_pass(self):
+        """seed_and_filter_all over the swapped-in query, plain per-chunk form."""
+        out, n, st = C.c_void_p(), C.c_uint64(), N.StatsC()
+        N.check(N.lib().hz_run_pass(self._h, C.byref(out), C.byref(n), C.byref(st)))
+        return _take(out, n.value, PASS_RECORD), st.as_dict()
+
+    # --- profiling ----------------------------------------------------------
+    def set_profiling(self, on: bool = True):
+        N.check(N.lib().hz_engine_set_profiling(self._h, int(bool(on))))
+
+    def profile(self):
+        out = {}
+        i = 0
+        name = C.create_string_buffer(128)
+        ms, n = C.c_double(), C.c_uint64()
+        while N.lib().hz_engine_profile_entry(self._h, i, name, 128, C.byref(ms), C.byref(n)) == 0:
+            out[name.value.decode()] = (ms.value, n.value)
+            i += 1
+        return out
+
+    def profile_reset(self):
+        N.check(N.lib().hz_engine_profile_reset(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(N.lib().hz_engine_launches(self._h))
+
+
+def dedup_and_order(h: np.ndarray) -> np.ndarray:
+    """dedup_and_order (src/hsp.rs:94-126) through the library's host code."""
+    a = np.ascontiguousarray(h, dtype=SEGMENT_PAIR).copy()
+    k = C.c_uint64()
+    N.check(N.lib().hz_dedup_and_order(_ptr(a), a.size, C.byref(k)))
+    return a[: k.value]

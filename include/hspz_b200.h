@@ -1,0 +1,150 @@
+/*
+ * hspz_b200.h -- C ABI of the B200 seed-and-filter engine.
+ *
+ * Plain pointers and sizes only; every entry point returns 0 or a negative
+ * HZ_E_* code and leaves a message in hz_last_error() (thread-local).  An
+ * engine is single-threaded (like the reference's Engine, one per worker
+ * thread) and owns all of its device memory.  There is no CPU fallback: on a
+ * machine without a usable sm_100 device hz_engine_create fails with
+ * HZ_E_CUDA.
+ *
+ * Each entry point names the reference interface it replaces (hspZ, Rust).
+ */
+#ifndef HSPZ_B200_H
+#define HSPZ_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HZ_OK 0
+#define HZ_E_STATE (-1)    /* call order violated (e.g. no query swapped in) */
+#define HZ_E_CUDA (-5)     /* CUDA runtime error */
+#define HZ_E_OOM (-12)     /* device or host allocation failed */
+#define HZ_E_INVALID (-22) /* bad argument */
+#define HZ_E_BUDGET (-28)  /* serving admission budget exceeded */
+#define HZ_E_TIMEOUT (-110)
+
+/* SegmentPair (src/hsp.rs:31-41): block-relative starts, extent, score. */
+typedef struct hz_segment_pair {
+  uint32_t ref_start;
+  uint32_t query_start;
+  uint32_t len;
+  int32_t score;
+} hz_segment_pair;
+
+/* One record of a pass: LASTZ interval index, strand (0 '+', 1 '-'). */
+typedef struct hz_pass_record {
+  uint32_t interval;
+  uint32_t strand;
+  hz_segment_pair h;
+} hz_pass_record;
+
+/* EngineConfig (src/gpu/mod.rs:1005-1019) plus the run flags that
+ * parameterise the path (src/cli.rs:41-183). */
+typedef struct hz_config {
+  int32_t sub_mat[64];   /* build_sub_mat (src/scoring.rs:41-120), device alphabet */
+  char seed[64];         /* "12of19", "14of22" or a 1/0/T pattern (Shape::parse) */
+  int32_t xdrop;         /* -x, 910 */
+  int32_t hspthresh;     /* -H, 3000 */
+  uint32_t noentropy;    /* -E */
+  uint32_t transitions;  /* 1 unless --notransition */
+  uint32_t step;         /* -e, seed-table step, 1 */
+  uint32_t max_hits;     /* --max-hits; 0 derives 4194304 x device GiB (src/gpu/mod.rs:2422-2442) */
+  uint32_t occ_cap;      /* per-seed occurrence cap, 0 = none (an extension of this build) */
+  uint32_t wga_chunk;    /* -C, 250000 */
+  uint32_t interval;     /* -I, 10000000 */
+  uint32_t strand;       /* 1 plus, 2 minus, 3 both (-S) */
+} hz_config;
+
+/* Counters of one call or pass (FilterOutput, src/gpu/mod.rs:55-67). */
+typedef struct hz_stats {
+  uint64_t seeds;     /* seeds generated (valid windows x variants) */
+  uint64_t hits;      /* seed hits expanded, after the occurrence cap */
+  uint64_t raw_hsps;  /* HSPs above threshold before dedup */
+  uint64_t hsps;      /* HSPs after dedup */
+  uint64_t cells;     /* scalar X-drop cells scored, both directions */
+  uint64_t calls;     /* seed_and_filter calls that had seeds */
+} hz_stats;
+
+typedef struct hz_engine hz_engine;
+
+const char *hz_last_error(void);
+void hz_free(void *p);
+
+/* Shape::parse (src/seed.rs:49-79): width and care-position count. */
+int hz_shape_info(const char *seed, uint32_t *size, uint32_t *kmer_size);
+
+/* Engine::new minus the tables (src/gpu/mod.rs:1021-1128): binds `device`,
+ * creates the engine's stream and loads the configuration. */
+int hz_engine_create(const hz_config *cfg, int device, hz_engine **out);
+void hz_engine_destroy(hz_engine *e);
+
+/* Engine::new's tables as the reference builds them on the host
+ * (EngineConfig.index_table / pos_table / ref_seq, src/gpu/mod.rs:1005-1011,
+ * built by SeedTable::build_parallel src/seed.rs:207-363). ref_seq is in the
+ * device alphabet. */
+int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t index_len,
+                          const uint32_t *pos_table, uint64_t pos_len, const uint8_t *ref_seq,
+                          uint64_t ref_len);
+
+/* The same target built on the device from the ASCII reference block:
+ * encode (src/sequence.rs:66-79) + SeedTable::build (src/seed.rs:135-180),
+ * byte-identical tables, resident until the next load. */
+int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len);
+
+/* Copies the resident seed table back (tests / interop): index_len entries
+ * of index_table and *pos_len of pos_table (pass NULL to query sizes). */
+int hz_engine_read_tables(hz_engine *e, uint32_t *index_table, uint64_t *index_len, uint32_t *pos_table,
+                          uint64_t *pos_len);
+
+/* Engine::swap_query (src/gpu/mod.rs:1142-1148): both strands already in
+ * the device alphabet. */
+int hz_swap_query(hz_engine *e, const uint8_t *query, const uint8_t *query_rc, uint64_t len);
+
+/* swap_query from the ASCII query block: the forward and reverse-complement
+ * encodings are made on the device (src/sequence.rs:66-86, 212-230). */
+int hz_swap_query_ascii(hz_engine *e, const uint8_t *query_ascii, uint64_t len);
+
+/* Engine::upload_seeds (src/gpu/mod.rs:1246): seeds kmer << 32 | position. */
+int hz_upload_seeds(hz_engine *e, uint32_t slot, const uint64_t *seeds, uint64_t n);
+
+/* Engine::generate_seeds (src/gpu/mod.rs:1312-1463): the seeds of query
+ * positions [start, end) of one strand, made and looked up on the device;
+ * *n_seeds as chunk_seeds would return. */
+int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint32_t end, int transitions,
+                      uint64_t *n_seeds);
+
+/* Engine::seed_and_filter (src/gpu/mod.rs:1499-2178): lookup, MAX_HITS
+ * chunking, expansion, X-drop extension, entropy, and per-chunk
+ * dedup_and_order; *out (hz_free) is deduped per chunk, LASTZ order,
+ * concatenated.  HZ_E_STATE without a swapped-in query. */
+int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **out, uint64_t *n,
+                       hz_stats *stats);
+
+/* seed_and_filter_all (src/run.rs:266-495), plain per-chunk form: every
+ * interval x strand x WGA chunk of the swapped-in query, one launch chain per
+ * call.  Records are grouped per interval, plus before minus, in call order. */
+int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats);
+
+/* dedup_and_order (src/hsp.rs:94-126) on host records, in place; returns
+ * the kept count in *n_out. */
+int hz_dedup_and_order(hz_segment_pair *h, uint64_t n, uint64_t *n_out);
+
+/* Per-kernel device time (CUDA events on the engine's stream) since the last
+ * reset; enable with hz_engine_set_profiling.  Entry i: name, total ms,
+ * launches.  Returns HZ_E_INVALID past the last entry. */
+int hz_engine_set_profiling(hz_engine *e, int on);
+int hz_engine_profile_entry(hz_engine *e, uint32_t i, char *name, uint32_t name_cap, double *ms,
+                            uint64_t *launches);
+int hz_engine_profile_reset(hz_engine *e);
+
+/* Kernel launches issued by this engine since creation. */
+uint64_t hz_engine_launches(hz_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
