@@ -86,6 +86,7 @@ SIGNATURES = {
     "hz_engine_profile_entry": (C.c_int, [P, U32, C.c_char_p, U32, C.POINTER(C.c_double), PU64]),
     "hz_engine_profile_reset": (C.c_int, [P]),
     "hz_engine_launches": (U64, [P]),
+    "hz_engine_set_stream": (C.c_int, [P, P]),
 }
 
 

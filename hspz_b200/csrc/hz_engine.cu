@@ -195,6 +195,7 @@ struct ProfEntry {
 struct hz_engine {
   int device = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t own_st = nullptr;
   hz_config cfg;
   ShapeDev shape;
   ExtendParams ep;
@@ -503,11 +504,12 @@ int hz_engine_create(const hz_config *cfg, int device, hz_engine **out) {
     uint64_t m = (uint64_t)v;
     e->max_hits = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(m, 1), 0xFFFFFFFFull);
   }
-  cudaError_t se = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+  cudaError_t se = cudaStreamCreateWithFlags(&e->own_st, cudaStreamNonBlocking);
   if (se != cudaSuccess) {
     delete e;
     return fail(HZ_E_CUDA, "stream: %s", cudaGetErrorString(se));
   }
+  e->st = e->own_st;
   uint8_t t_enc[256], t_rc[256];
   for (int c = 0; c < 256; c++) {
     t_enc[c] = enc_of((uint8_t)c);
@@ -564,7 +566,7 @@ void hz_engine_destroy(hz_engine *e) {
     cudaEventDestroy(pe.second.second);
   }
   for (auto ev : e->event_pool) cudaEventDestroy(ev);
-  if (e->st) cudaStreamDestroy(e->st);
+  if (e->own_st) cudaStreamDestroy(e->own_st);
   delete e;
 }
 
@@ -938,5 +940,13 @@ int hz_engine_profile_reset(hz_engine *e) {
 }
 
 uint64_t hz_engine_launches(hz_engine *e) { return e ? e->launches : 0; }
+
+int hz_engine_set_stream(hz_engine *e, void *stream) {
+  if (!e) return fail(HZ_E_INVALID, "null engine");
+  TRY(set_device(e));
+  TRY(e->sync());
+  e->st = stream ? (cudaStream_t)stream : e->own_st;
+  return HZ_OK;
+}
 
 }  // extern "C"

@@ -178,6 +178,11 @@ class Engine:
     def profile_reset(self):
         N.check(N.lib().hz_engine_profile_reset(self._h))
 
+    def set_stream(self, stream_handle: int):
+        """Run on a caller-owned cudaStream_t (an int handle, e.g.
+        torch.cuda.current_stream().cuda_stream); 0 restores the own stream."""
+        N.check(N.lib().hz_engine_set_stream(self._h, C.c_void_p(stream_handle or None)))
+
     @property
     def launches(self) -> int:
         return int(N.lib().hz_engine_launches(self._h))

@@ -144,6 +144,10 @@ int hz_engine_profile_reset(hz_engine *e);
 /* Kernel launches issued by this engine since creation. */
 uint64_t hz_engine_launches(hz_engine *e);
 
+/* Runs the engine's work on a caller-owned cudaStream_t (NULL restores the
+ * engine's own stream), so callers can order and time it with their events. */
+int hz_engine_set_stream(hz_engine *e, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
