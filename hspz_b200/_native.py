@@ -52,12 +52,7 @@ class StatsC(C.Structure):
 
 
 class QueryC(C.Structure):
-    _fields_ = [("ascii", C.c_void_p), ("len", C.c_uint64), ("id", C.c_uint32), ("_pad", C.c_uint32)]
-
-
-class BatchRecordC(C.Structure):
-    _fields_ = [("query", C.c_uint32), ("interval", C.c_uint32), ("strand", C.c_uint32), ("_pad", C.c_uint32),
-                ("h", SegmentPairC)]
+    _fields_ = [("ascii", C.c_void_p), ("len", C.c_uint64)]
 
 
 _lib = None
@@ -82,11 +77,14 @@ SIGNATURES = {
     "hz_seed_and_filter": (C.c_int, [P, U32, C.c_int, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_run_pass": (C.c_int, [P, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_dedup_and_order": (C.c_int, [P, U64, PU64]),
+    "hz_stage_queries": (C.c_int, [P, C.POINTER(QueryC), U32]),
+    "hz_run_batched": (C.c_int, [P, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_engine_set_profiling": (C.c_int, [P, C.c_int]),
     "hz_engine_profile_entry": (C.c_int, [P, U32, C.c_char_p, U32, C.POINTER(C.c_double), PU64]),
     "hz_engine_profile_reset": (C.c_int, [P]),
     "hz_engine_launches": (U64, [P]),
     "hz_engine_set_stream": (C.c_int, [P, P]),
+    "hz_engine_set_tuning": (C.c_int, [P, C.c_char_p, C.c_int64]),
 }
 
 

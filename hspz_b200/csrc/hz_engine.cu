@@ -1,7 +1,12 @@
 // Host side of the B200 seed-and-filter engine and its C ABI
-// (include/hspz_b200.h).  One engine = one device, one stream, resident
-// target tables, the swapped-in query and two seed slots, mirroring the
-// reference's Engine (src/gpu/mod.rs:817-2307).
+// (include/hspz_b200.h).  One engine = one device, one stream, a resident
+// target (reference codes, index_table, pos_table), a resident query store
+// and two seed slots, mirroring the reference's Engine (src/gpu/mod.rs:817-2307).
+//
+// Every seed_and_filter call goes through the same wave pipeline
+// (hz_wave.cuh).  The plain per-chunk form runs one call per wave and reads
+// its HSPs back after each call, as the reference does; the batched form runs
+// many calls per wave with one read-back per wave.
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -14,6 +19,7 @@
 #include "../../include/hspz_b200.h"
 #include "hz_kernels.cuh"
 #include "hz_scan.cuh"
+#include "hz_wave.cuh"
 
 using namespace hz;
 
@@ -39,11 +45,13 @@ int fail(int code, const char *fmt, ...) {
                   cudaGetErrorString(e_), __FILE__, __LINE__);                                 \
   } while (0)
 
-#define TRY(x)                \
-  do {                        \
-    int r_ = (x);             \
+#define TRY(x)                  \
+  do {                          \
+    int r_ = (x);               \
     if (r_ != HZ_OK) return r_; \
   } while (0)
+
+constexpr size_t kPad = 64;  // bytes of padding before and after every sequence buffer
 
 // Grow-only device buffer.  Growing waits for the stream, because a queued
 // kernel may still read the old allocation.
@@ -51,8 +59,9 @@ template <typename T> struct DBuf {
   T *p = nullptr;
   size_t cap = 0;
   int ensure(size_t n, cudaStream_t s) {
-    if (n <= cap) return HZ_OK;
+    if (n <= cap && p) return HZ_OK;
     size_t want = std::max(n, cap + cap / 2);
+    if (want == 0) want = 1;
     if (p) {
       CK(cudaStreamSynchronize(s));
       CK(cudaFree(p));
@@ -75,8 +84,9 @@ template <typename T> struct HBuf {
   T *p = nullptr;
   size_t cap = 0;
   int ensure(size_t n) {
-    if (n <= cap) return HZ_OK;
+    if (n <= cap && p) return HZ_OK;
     size_t want = std::max(n, cap + cap / 2);
+    if (want == 0) want = 1;
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
@@ -88,6 +98,21 @@ template <typename T> struct HBuf {
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
+  }
+};
+
+// A sequence buffer with kPad zero bytes on both sides (word loads of the
+// extension kernels may touch them; their cells are never scored).
+struct SeqBuf {
+  DBuf<uint8_t> buf;
+  size_t len = 0;
+  uint8_t *base() const { return buf.p + kPad; }
+  int ensure(size_t n, cudaStream_t s) {
+    TRY(buf.ensure(n + 2 * kPad, s));
+    CK(cudaMemsetAsync(buf.p, 0, kPad, s));
+    CK(cudaMemsetAsync(buf.p + kPad + n, 0, kPad, s));
+    len = n;
+    return HZ_OK;
   }
 };
 
@@ -176,15 +201,27 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148u * 64u) {
 
 // ---------------------------------------------------------------------------
 
+// One call as the host sees it: a WGA chunk [start, end) of one strand of one
+// staged query, tagged with its LASTZ interval.
+struct HostCall {
+  uint32_t query;
+  uint32_t interval;
+  uint32_t strand;  // 0 forward, 1 reverse complement
+  uint32_t start, end;
+};
+
+// A staged query block: forward and reverse-complement codes in the store.
+struct StagedQuery {
+  uint32_t off_f = 0, off_r = 0, len = 0;
+};
+
 struct Slot {
-  int kind = 0;  // 0 empty, 1 uploaded seeds, 2 generated on device
+  int kind = 0;  // 0 empty, 1 uploaded seeds, 2 generated range
   DBuf<uint64_t> seeds;
-  uint64_t n_slots = 0;  // seed slots of the call (uploaded: seeds; generated: span * per_pos)
-  uint64_t n_seeds = 0;  // real seeds (chunk_seeds count)
+  uint64_t n = 0;
   int rev = 0;
-  uint32_t start = 0, end = 0, per_pos = 1;
-  DBuf<uint32_t> cnt, bst;
-  bool counted = false;
+  uint32_t start = 0, end = 0;
+  int transitions = 1;
 };
 
 struct ProfEntry {
@@ -192,36 +229,52 @@ struct ProfEntry {
   uint64_t n = 0;
 };
 
+// One output record of a wave: the call and the HSP (after per-scope dedup).
+struct WaveRecord {
+  uint32_t call;
+  hz_segment_pair h;
+};
+
 struct hz_engine {
   int device = 0;
+  int sm_count = 148;
   cudaStream_t st = nullptr;
   cudaStream_t own_st = nullptr;
   hz_config cfg;
   ShapeDev shape;
-  ExtendParams ep;
   uint32_t max_hits = 0;
   // target
-  DBuf<uint8_t> ref;
+  SeqBuf ref;
   uint32_t rlen = 0;
   DBuf<uint32_t> index_table;
   uint64_t index_len = 0;
   DBuf<uint32_t> pos_table;
   uint64_t n_pos = 0;
   bool has_target = false;
-  // query
-  DBuf<uint8_t> qf, qr, qascii;
-  uint32_t qlen = 0;
+  // query store
+  SeqBuf qstore;
+  DBuf<uint8_t> qascii;
+  std::vector<StagedQuery> queries;
   bool has_query = false;
   Slot slot[2];
-  // per-call work
-  DBuf<uint2> pairs, pair_partial, pair_total;
-  DBuf<uint32_t> c_incl, c_qpos, c_bst, bounds, status, raw_count, bad;
-  DBuf<uint64_t> anchors;
+  // wave buffers
+  DBuf<CallDev> calls;
+  DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope;
+  DBuf<unsigned long long> np_excl, call_hit_lo, scope_lo;
+  DBuf<HitNz> np_partial, np_grand;
+  DBuf<WaveTotals> tot;
+  DBuf<Cand> cand;
   DBuf<SegmentPair> raw;
-  DBuf<unsigned long long> cells, n_valid;
-  HBuf<uint8_t> h_stage;
+  HBuf<CallDev> h_calls;
+  HBuf<WaveTotals> h_tot;
   HBuf<hz_segment_pair> h_raw;
-  HBuf<uint32_t> h_small;
+  HBuf<uint32_t> h_raw_scope, h_scope_call;
+  uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
+  // tuning
+  int gate_tile = 2048;
+  uint32_t gate_cap = 256;
+  int gate_blocks_per_sm = 0;
+  uint64_t wave_positions = 1ull << 27;  // seed positions per batched wave
   // profiling
   bool profiling = false;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
@@ -240,8 +293,9 @@ struct hz_engine {
     cudaEventCreate(&e);
     return e;
   }
-  // Brackets one launch with events when profiling.
-  template <typename F> int launch(const char *name, F &&f) {
+  // Brackets one launch (or launch group counted as `count` kernels) with
+  // events when profiling.
+  template <typename F> int launch(const char *name, F &&f, int count = 1) {
     cudaEvent_t a = nullptr, b = nullptr;
     if (profiling) {
       a = get_event();
@@ -249,7 +303,7 @@ struct hz_engine {
       cudaEventRecord(a, st);
     }
     f();
-    launches++;
+    launches += count;
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return fail(HZ_E_CUDA, "launch %s: %s", name, cudaGetErrorString(err));
     if (profiling) {
@@ -273,6 +327,7 @@ struct hz_engine {
     pending.clear();
     return HZ_OK;
   }
+  uint32_t per_pos(int transitions) const { return transitions ? 1 + shape.kmer_size : 1; }
 };
 
 namespace {
@@ -282,161 +337,267 @@ int set_device(hz_engine *e) {
   return HZ_OK;
 }
 
-// Exclusive scan of the (hits, non-empty) pairs of n seed slots; totals to
-// host: *num_hits and *n_entries.
-int scan_pairs(hz_engine *e, const uint32_t *cnt, uint64_t n, uint64_t *num_hits, uint64_t *n_entries) {
-  TRY(e->pairs.ensure(n, e->st));
-  TRY(e->pair_partial.ensure(scan_tiles(n) + 1, e->st));
-  TRY(e->pair_total.ensure(1, e->st));
-  uint2 *pairs = e->pairs.p;
-  TRY(e->launch("pair", [&] { pair_kernel<<<grid_for(n, 256), 256, 0, e->st>>>(cnt, n, pairs); }));
-  TRY(e->launch("scan", [&] {
-    exclusive_scan<uint2>(pairs, pairs, n, e->pair_partial.p, e->pair_total.p, e->st);
-  }));
-  e->launches += 2;
-  TRY(e->h_small.ensure(4));
-  CK(cudaMemcpyAsync(e->h_small.p, e->pair_total.p, sizeof(uint2), cudaMemcpyDeviceToHost, e->st));
-  TRY(e->sync());
-  *num_hits = e->h_small.p[0];
-  *n_entries = e->h_small.p[1];
-  return HZ_OK;
+template <int TILE> size_t gate_smem() { return sizeof(GateSmem<TILE>); }
+
+template <int TILE> int launch_gate(hz_engine *e, const GateArgs &ga) {
+  static bool configured[64] = {false};
+  size_t smem = gate_smem<TILE>();
+  if (!configured[e->device & 63]) {
+    CK(cudaFuncSetAttribute(gate_kernel<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured[e->device & 63] = true;
+  }
+  int per_sm = e->gate_blocks_per_sm;
+  if (per_sm <= 0) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate_kernel<TILE>, kScanThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  unsigned grid = (unsigned)(e->sm_count * per_sm);
+  return e->launch("gate", [&] { gate_kernel<TILE><<<grid, kScanThreads, smem, e->st>>>(ga); });
 }
 
-// Everything after the seed lookup of one call: compaction, MAX_HITS walk,
-// per-chunk expansion + extension, per-chunk dedup.  Appends to `out`.
-int filter_slot(hz_engine *e, Slot &s, const uint8_t *qry, std::vector<hz_segment_pair> &out, hz_stats *st) {
-  uint64_t n = s.n_slots;
+// Runs calls[0..n) as one wave and appends its deduped HSPs, in call order
+// and LASTZ order within each MAX_HITS scope, to *out.  `seeds` (device) is
+// the uploaded seed array of a single-call wave, or null.
+int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, int transitions,
+             std::vector<WaveRecord> *out, hz_stats *st) {
   if (n == 0) return HZ_OK;
-  uint64_t num_hits64 = 0, n_entries = 0;
-  TRY(scan_pairs(e, s.cnt.p, n, &num_hits64, &n_entries));
-  if (st) {
-    st->hits += num_hits64;
-    st->seeds += s.n_seeds;
-    st->calls += 1;
+  cudaStream_t s = e->st;
+  uint64_t npos = 0;
+  TRY(e->h_calls.ensure(n));
+  for (size_t i = 0; i < n; i++) {
+    const StagedQuery &q = e->queries[hc[i].query];
+    CallDev &c = e->h_calls.p[i];
+    c.qoff = hc[i].strand ? q.off_r : q.off_f;
+    c.qlen = q.len;
+    c.start = hc[i].start;
+    c.pos_off = (uint32_t)npos;
+    npos += hc[i].end - hc[i].start;
   }
-  if (num_hits64 == 0) return HZ_OK;
-  if (num_hits64 > 0xFFFFFFFFull)
-    return fail(HZ_E_INVALID, "a call holds %llu seed hits; num_hits is a u32 in the reference",
-                (unsigned long long)num_hits64);
-  uint32_t num_hits = (uint32_t)num_hits64;
+  if (npos == 0) return HZ_OK;
+  if (npos >= 0x7FFFFFFFull) return fail(HZ_E_INVALID, "a wave of %llu seed positions exceeds 2^31", (unsigned long long)npos);
+  TRY(e->calls.ensure(n, s));
+  TRY(e->pos_hits.ensure(npos, s));
+  uint64_t tiles = scan_tiles(npos);
+  TRY(e->np_partial.ensure(tiles + 1, s));
+  TRY(e->np_grand.ensure(1, s));
+  TRY(e->np_excl.ensure(npos + 1, s));
+  TRY(e->np_pos.ensure(npos + 1, s));
+  TRY(e->call_hit_lo.ensure(n + 1, s));
+  TRY(e->call_nz_lo.ensure(n + 1, s));
+  TRY(e->tot.ensure(1, s));
+  TRY(e->h_tot.ensure(1));
+  CK(cudaMemcpyAsync(e->calls.p, e->h_calls.p, n * sizeof(CallDev), cudaMemcpyHostToDevice, s));
 
-  TRY(e->c_incl.ensure(n_entries, e->st));
-  TRY(e->c_qpos.ensure(n_entries, e->st));
-  TRY(e->c_bst.ensure(n_entries, e->st));
-  const uint64_t *up = s.kind == 1 ? s.seeds.p : nullptr;
-  TRY(e->launch("seed_compact", [&] {
-    seed_compact_kernel<<<grid_for(n, 256), 256, 0, e->st>>>(s.cnt.p, s.bst.p, e->pairs.p, n, s.per_pos, s.start,
-                                                              up, e->c_incl.p, e->c_qpos.p, e->c_bst.p);
-  }));
+  WaveIn w;
+  w.ref = e->ref.base();
+  w.rlen = e->rlen;
+  w.qbuf = e->qstore.base();
+  w.index_table = e->index_table.p;
+  w.pos_table = e->pos_table.p;
+  w.calls = e->calls.p;
+  w.ncalls = (uint32_t)n;
+  w.npos = (uint32_t)npos;
+  w.seeds = seeds;
+  w.shape = e->shape;
+  w.per_pos = seeds ? 1u : e->per_pos(transitions);
+  w.occ_cap = e->cfg.occ_cap;
 
-  // chunk bounds in hit space
-  std::vector<uint32_t> bounds;
-  if (num_hits <= e->max_hits) {
-    bounds = {0u, num_hits};
-  } else {
-    uint32_t num_iter = num_hits / e->max_hits + 1;
-    TRY(e->bounds.ensure(num_iter + 1, e->st));
-    TRY(e->status.ensure(1, e->st));
-    // first real seed: the first slot with a bucket
-    uint32_t first_hits = 0;
-    {
-      std::vector<uint32_t> hb;
-      // scan forward on the host in blocks; this path only runs when a call
-      // exceeds max_hits
-      const uint64_t blk = 1 << 16;
-      bool found = false;
-      std::vector<uint32_t> c(blk), b(blk);
-      for (uint64_t off = 0; off < n && !found; off += blk) {
-        uint64_t m = std::min<uint64_t>(blk, n - off);
-        CK(cudaMemcpyAsync(c.data(), s.cnt.p + off, m * 4, cudaMemcpyDeviceToHost, e->st));
-        CK(cudaMemcpyAsync(b.data(), s.bst.p + off, m * 4, cudaMemcpyDeviceToHost, e->st));
-        TRY(e->sync());
-        for (uint64_t i = 0; i < m; i++)
-          if (b[i] != kNoBucket) {
-            first_hits = c[i];
-            found = true;
-            break;
-          }
-      }
+  for (int attempt = 0; attempt < 4; attempt++) {
+    uint32_t scope_cap = std::max<uint32_t>(e->scope_cap, (uint32_t)n * 2 + 16);
+    TRY(e->scope_lo.ensure(scope_cap + 1, s));
+    TRY(e->scope_call.ensure(scope_cap + 1, s));
+    TRY(e->cand.ensure(e->cand_cap, s));
+    TRY(e->raw.ensure(e->raw_cap, s));
+    TRY(e->raw_scope.ensure(e->raw_cap, s));
+    CK(cudaMemsetAsync(e->tot.p, 0, sizeof(WaveTotals), s));
+
+    TRY(e->launch("lookup_count", [&] {
+      lookup_count_kernel<<<(unsigned)((npos + kCountPerBlock - 1) / kCountPerBlock), kCountThreads, 0, s>>>(
+          w, e->pos_hits.p, e->tot.p);
+    }));
+    TRY(e->launch(
+        "np_scan",
+        [&] {
+          np_reduce_kernel<<<(unsigned)tiles, kScanThreads, 0, s>>>(e->pos_hits.p, npos, e->np_partial.p);
+          scan_partials_kernel<HitNz><<<1, kScanThreads, 0, s>>>(e->np_partial.p, tiles, e->np_grand.p);
+          np_emit_kernel<<<(unsigned)tiles, kScanThreads, 0, s>>>(e->pos_hits.p, npos, e->np_partial.p,
+                                                                  e->np_excl.p, e->np_pos.p);
+          np_totals_kernel<<<1, 32, 0, s>>>(e->np_grand.p, e->tot.p, e->np_excl.p);
+        },
+        4));
+    TRY(e->launch("scopes", [&] {
+      scopes_kernel<<<1, kScopeThreads, 0, s>>>(w, e->np_excl.p, e->np_pos.p, e->tot.p, e->max_hits,
+                                                e->call_hit_lo.p, e->call_nz_lo.p, e->scope_lo.p, e->scope_call.p,
+                                                scope_cap);
+    }));
+    GateArgs ga;
+    ga.w = w;
+    ga.np_excl = e->np_excl.p;
+    ga.np_pos = e->np_pos.p;
+    ga.scope_lo = e->scope_lo.p;
+    ga.scope_cap = scope_cap;
+    ga.tot = e->tot.p;
+    memcpy(ga.sub, e->cfg.sub_mat, sizeof(ga.sub));
+    ga.xdrop = e->cfg.xdrop;
+    ga.hspthresh = e->cfg.hspthresh;
+    ga.cap = e->gate_cap;
+    ga.cand = e->cand.p;
+    ga.cand_cap = e->cand_cap;
+    switch (e->gate_tile) {
+      case 1024: TRY(launch_gate<1024>(e, ga)); break;
+      case 4096: TRY(launch_gate<4096>(e, ga)); break;
+      default: TRY(launch_gate<2048>(e, ga)); break;
     }
-    uint32_t *bp = e->bounds.p, *sp = e->status.p;
-    TRY(e->launch("chunk_walk", [&] {
-      chunk_walk_kernel<<<1, 32, 0, e->st>>>(e->c_incl.p, (uint32_t)n_entries, num_hits, e->max_hits, first_hits, bp,
-                                             sp);
+    ExactArgs xa;
+    xa.ref = w.ref;
+    xa.rlen = w.rlen;
+    xa.qbuf = w.qbuf;
+    xa.calls = w.calls;
+    xa.cand = e->cand.p;
+    xa.cand_cap = e->cand_cap;
+    xa.tot = e->tot.p;
+    memcpy(xa.sub, e->cfg.sub_mat, sizeof(xa.sub));
+    xa.xdrop = e->cfg.xdrop;
+    xa.hspthresh = e->cfg.hspthresh;
+    xa.noentropy = e->cfg.noentropy ? 1u : 0u;
+    xa.raw = e->raw.p;
+    xa.raw_scope = e->raw_scope.p;
+    xa.raw_cap = e->raw_cap;
+    TRY(e->launch("exact", [&] {
+      exact_kernel<<<(unsigned)(e->sm_count * 8), kExactThreads, 0, s>>>(xa);
     }));
-    bounds.resize(num_iter + 1);
-    uint32_t status = 0;
-    CK(cudaMemcpyAsync(bounds.data(), bp, (num_iter + 1) * 4, cudaMemcpyDeviceToHost, e->st));
-    CK(cudaMemcpyAsync(&status, sp, 4, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaMemcpyAsync(e->h_tot.p, e->tot.p, sizeof(WaveTotals), cudaMemcpyDeviceToHost, s));
     TRY(e->sync());
-    if (status)
-      return fail(HZ_E_INVALID, "the first seed of a call holds more than max_hits=%u hits; the reference's "
-                                "MAX_HITS walk has no valid cut there", e->max_hits);
-  }
+    WaveTotals t = *e->h_tot.p;
+    if (t.status & 2u) return fail(HZ_E_INVALID, "a call holds 2^32 or more seed hits; num_hits is a u32 in the reference");
+    if (t.status & 1u)
+      return fail(HZ_E_INVALID, "the first seed of a call holds more than max_hits=%u hits; the reference's MAX_HITS "
+                                "walk has no valid cut there", e->max_hits);
+    bool again = false;
+    if (t.n_scopes > scope_cap) {
+      e->scope_cap = t.n_scopes + 16;
+      again = true;
+    }
+    if (t.cand > e->cand_cap) {
+      e->cand_cap = t.cand + t.cand / 4 + 1024;
+      again = true;
+    }
+    if (t.raw > e->raw_cap) {
+      e->raw_cap = t.raw + t.raw / 4 + 1024;
+      again = true;
+    }
+    if (again) continue;  // a capacity was too small: run the wave again with larger buffers
 
-  for (size_t c = 0; c + 1 < bounds.size(); c++) {
-    uint32_t lo = bounds[c], hi = bounds[c + 1];
-    if (hi <= lo) continue;
-    uint32_t nh = hi - lo;
-    TRY(e->anchors.ensure(nh, e->st));
-    TRY(e->raw.ensure(nh, e->st));
-    TRY(e->raw_count.ensure(1, e->st));
-    CK(cudaMemsetAsync(e->raw_count.p, 0, 4, e->st));
-    uint64_t *an = e->anchors.p;
-    TRY(e->launch("expand", [&] {
-      expand_kernel<<<(nh + kExpandTile - 1) / kExpandTile, kExpandThreads, 0, e->st>>>(
-          e->c_incl.p, e->c_qpos.p, e->c_bst.p, (uint32_t)n_entries, e->pos_table.p, lo, hi, e->shape.size, an);
-    }));
-    ExtendParams ep = e->ep;
-    ep.qlen = e->qlen;
-    TRY(e->launch("extend", [&] {
-      extend_kernel<<<grid_for(nh, kExtendThreads, 148u * 16u), kExtendThreads, 0, e->st>>>(
-          e->ref.p, qry, an, nh, ep, e->raw.p, nh, e->raw_count.p, e->cells.p);
-    }));
-    uint32_t nraw = 0;
-    CK(cudaMemcpyAsync(&nraw, e->raw_count.p, 4, cudaMemcpyDeviceToHost, e->st));
-    TRY(e->sync());
-    if (nraw == 0) continue;
-    TRY(e->h_raw.ensure(nraw));
-    CK(cudaMemcpyAsync(e->h_raw.p, e->raw.p, (size_t)nraw * sizeof(hz_segment_pair), cudaMemcpyDeviceToHost,
-                       e->st));
-    TRY(e->sync());
-    size_t kept = dedup_and_order(e->h_raw.p, nraw);
-    out.insert(out.end(), e->h_raw.p, e->h_raw.p + kept);
+    // per-scope dedup on the host, in scope order
+    uint32_t nraw = t.raw;
     if (st) {
+      st->hits += t.hits;
+      st->cells += t.cells;
+      st->seeds += t.valid * w.per_pos;
       st->raw_hsps += nraw;
-      st->hsps += kept;
+      st->calls += n;
     }
+    if (nraw == 0) return HZ_OK;
+    TRY(e->h_raw.ensure(nraw));
+    TRY(e->h_raw_scope.ensure(nraw));
+    TRY(e->h_scope_call.ensure(t.n_scopes + 1));
+    CK(cudaMemcpyAsync(e->h_raw.p, e->raw.p, (size_t)nraw * sizeof(SegmentPair), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_raw_scope.p, e->raw_scope.p, (size_t)nraw * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_scope_call.p, e->scope_call.p, (size_t)t.n_scopes * 4, cudaMemcpyDeviceToHost, s));
+    TRY(e->sync());
+    // counting sort by scope
+    std::vector<uint32_t> start(t.n_scopes + 1, 0);
+    for (uint32_t i = 0; i < nraw; i++) start[e->h_raw_scope.p[i] + 1]++;
+    for (uint32_t k = 0; k < t.n_scopes; k++) start[k + 1] += start[k];
+    std::vector<hz_segment_pair> sorted(nraw);
+    std::vector<uint32_t> cur(start.begin(), start.end() - 1);
+    for (uint32_t i = 0; i < nraw; i++) sorted[cur[e->h_raw_scope.p[i]]++] = e->h_raw.p[i];
+    for (uint32_t k = 0; k < t.n_scopes; k++) {
+      size_t a = start[k], b = start[k + 1];
+      if (a == b) continue;
+      size_t kept = dedup_and_order(sorted.data() + a, b - a);
+      if (st) st->hsps += kept;
+      uint32_t c = e->h_scope_call.p[k];
+      for (size_t i = 0; i < kept; i++) out->push_back(WaveRecord{c, sorted[a + i]});
+    }
+    return HZ_OK;
   }
-  return HZ_OK;
+  return fail(HZ_E_OOM, "wave buffers kept overflowing");
 }
 
-// Device seed lookup for positions [start, end) of one strand into slot s.
-int generate_into(hz_engine *e, Slot &s, int rev, uint32_t start, uint32_t end, int transitions) {
-  s.kind = 2;
-  s.rev = rev;
-  s.start = start;
-  s.end = end;
-  s.per_pos = transitions ? 1 + e->shape.kmer_size : 1;
-  uint32_t span = end > start ? end - start : 0;
-  s.n_slots = (uint64_t)span * s.per_pos;
-  s.counted = true;
-  if (span == 0) return HZ_OK;
-  TRY(s.cnt.ensure(s.n_slots, e->st));
-  TRY(s.bst.ensure(s.n_slots, e->st));
-  const uint8_t *q = rev ? e->qr.p : e->qf.p;
-  TRY(e->launch("seed_count", [&] {
-    seed_count_kernel<<<grid_for(span, 256), 256, 0, e->st>>>(q, start, span, s.per_pos, e->shape,
-                                                              e->index_table.p, e->cfg.occ_cap, s.cnt.p, s.bst.p,
-                                                              e->n_valid.p);
-  }));
+// The calls of one staged query in the reference's batch order: per LASTZ
+// interval (src/sequence.rs:322-334), the plus WGA chunks then the minus
+// chunks over (qbl - end, qbl - start) (src/run.rs:278-299, chunks
+// src/seed.rs:488-496).
+void query_calls(const hz_engine *e, uint32_t qid, std::vector<HostCall> *out) {
+  uint64_t qlen = e->queries[qid].len;
+  uint32_t ss = e->shape.size;
+  if (qlen <= ss) return;
+  uint32_t end_pos = (uint32_t)(qlen - ss), qbl = end_pos;
+  uint32_t iv = 0;
+  for (uint64_t cur = 0; cur < end_pos; cur += e->cfg.interval, iv++) {
+    uint32_t is = (uint32_t)cur, ie = (uint32_t)std::min<uint64_t>(end_pos, cur + e->cfg.interval);
+    for (uint32_t rev = 0; rev < 2; rev++) {
+      if (!(e->cfg.strand & (1u << rev))) continue;
+      uint32_t a = rev ? qbl - ie : is, b = rev ? qbl - is : ie;
+      for (uint64_t c = a; c < b; c += e->cfg.wga_chunk)
+        out->push_back(HostCall{qid, iv, rev, (uint32_t)c, (uint32_t)std::min<uint64_t>(c + e->cfg.wga_chunk, (uint64_t)b + 1)});
+    }
+  }
+}
+
+// Replaces the query store with `nq` ASCII blocks; each is encoded forward
+// and reverse-complemented on the device.
+int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens, uint32_t nq) {
+  uint64_t total = 0;
+  std::vector<StagedQuery> qs(nq);
+  for (uint32_t i = 0; i < nq; i++) {
+    if (lens[i] > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "query block %u exceeds u32 coordinates", i);
+    // every strand starts 16-byte aligned, with at least kPad bytes after it
+    qs[i].len = (uint32_t)lens[i];
+    qs[i].off_f = (uint32_t)total;
+    total = (total + lens[i] + kPad + 15) & ~15ull;
+    qs[i].off_r = (uint32_t)total;
+    total = (total + lens[i] + kPad + 15) & ~15ull;
+  }
+  if (total >= 0xFFFFFFFFull) return fail(HZ_E_INVALID, "staged queries exceed 4 GB");
+  cudaStream_t s = e->st;
+  TRY(e->qstore.ensure(total, s));
+  uint64_t maxlen = 0;
+  for (uint32_t i = 0; i < nq; i++) maxlen = std::max<uint64_t>(maxlen, lens[i]);
+  TRY(e->qascii.ensure(maxlen + 16, s));
+  CK(cudaMemsetAsync(e->qstore.base(), 0, total, s));
+  for (uint32_t i = 0; i < nq; i++) {
+    if (!lens[i]) continue;
+    CK(cudaMemcpyAsync(e->qascii.p, ascii[i], lens[i], cudaMemcpyHostToDevice, s));
+    uint8_t *f = e->qstore.base() + qs[i].off_f, *r = e->qstore.base() + qs[i].off_r;
+    uint64_t len = lens[i];
+    TRY(e->launch("encode", [&] {
+      encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, s>>>(e->qascii.p, len, f, r);
+    }));
+  }
+  TRY(e->sync());
+  e->queries = qs;
+  e->has_query = nq > 0;
+  e->slot[0].kind = e->slot[1].kind = 0;
   return HZ_OK;
 }
 
 int check_range(hz_engine *e, uint32_t start, uint32_t end) {
   if (end < start) return fail(HZ_E_INVALID, "seed range [%u, %u) is reversed", start, end);
-  if (end > start && (uint64_t)end + e->shape.size - 1 > e->qlen)
-    return fail(HZ_E_INVALID, "seed range [%u, %u) exceeds query length %u", start, end, e->qlen);
+  uint32_t qlen = e->queries.empty() ? 0 : e->queries[0].len;
+  if (end > start && (uint64_t)end + e->shape.size - 1 > qlen)
+    return fail(HZ_E_INVALID, "seed range [%u, %u) exceeds query length %u", start, end, qlen);
+  return HZ_OK;
+}
+
+int copy_out_segments(const std::vector<WaveRecord> &recs, hz_segment_pair **out, uint64_t *n) {
+  *out = nullptr;
+  *n = recs.size();
+  if (recs.empty()) return HZ_OK;
+  *out = (hz_segment_pair *)malloc(recs.size() * sizeof(hz_segment_pair));
+  if (!*out) return fail(HZ_E_OOM, "host allocation");
+  for (size_t i = 0; i < recs.size(); i++) (*out)[i] = recs[i].h;
   return HZ_OK;
 }
 
@@ -468,6 +629,7 @@ int hz_engine_create(const hz_config *cfg, int device, hz_engine **out) {
   memcpy(seed, cfg->seed, 64);
   seed[64] = 0;
   TRY(parse_shape(seed[0] ? seed : "12of19", &sh));
+  if (cfg->strand == 0 || cfg->strand > 3) return fail(HZ_E_INVALID, "strand must be 1 (plus), 2 (minus) or 3 (both)");
   int ndev = 0;
   cudaError_t err = cudaGetDeviceCount(&ndev);
   if (err != cudaSuccess || ndev == 0)
@@ -481,20 +643,13 @@ int hz_engine_create(const hz_config *cfg, int device, hz_engine **out) {
     return fail(HZ_E_CUDA, "device %d is sm_%d%d; this build targets sm_100a (B200)", device, prop.major, prop.minor);
   hz_engine *e = new hz_engine();
   e->device = device;
+  e->sm_count = prop.multiProcessorCount;
   e->cfg = *cfg;
   e->cfg.seed[63] = 0;
   e->shape = sh;
-  memcpy(e->ep.sub, cfg->sub_mat, sizeof(e->ep.sub));
-  e->ep.xdrop = cfg->xdrop;
-  e->ep.hspthresh = cfg->hspthresh;
-  e->ep.noentropy = cfg->noentropy ? 1u : 0u;
   if (e->cfg.step == 0) e->cfg.step = 1;
   if (e->cfg.wga_chunk == 0) e->cfg.wga_chunk = 250000;
   if (e->cfg.interval == 0) e->cfg.interval = 10000000;
-  if (e->cfg.strand == 0 || e->cfg.strand > 3) {
-    delete e;
-    return fail(HZ_E_INVALID, "strand must be 1 (plus), 2 (minus) or 3 (both)");
-  }
   if (cfg->max_hits > 0) {
     e->max_hits = cfg->max_hits;
   } else {
@@ -518,9 +673,8 @@ int hz_engine_create(const hz_config *cfg, int device, hz_engine **out) {
   int rc = HZ_OK;
   if (cudaMemcpyToSymbol(c_enc, t_enc, 256) != cudaSuccess || cudaMemcpyToSymbol(c_enc_rc, t_rc, 256) != cudaSuccess)
     rc = fail(HZ_E_CUDA, "constant tables: %s", cudaGetErrorString(cudaGetLastError()));
-  if (rc == HZ_OK) rc = e->cells.ensure(1, e->st);
-  if (rc == HZ_OK) rc = e->n_valid.ensure(1, e->st);
-  if (rc == HZ_OK && cudaMemsetAsync(e->cells.p, 0, 8, e->st) != cudaSuccess) rc = fail(HZ_E_CUDA, "memset");
+  if (rc == HZ_OK) rc = e->ref.ensure(0, e->st);
+  if (rc == HZ_OK) rc = e->qstore.ensure(0, e->st);
   if (rc != HZ_OK) {
     hz_engine_destroy(e);
     return rc;
@@ -533,34 +687,31 @@ void hz_engine_destroy(hz_engine *e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->st) cudaStreamSynchronize(e->st);
-  e->ref.release();
+  e->ref.buf.release();
   e->index_table.release();
   e->pos_table.release();
-  e->qf.release();
-  e->qr.release();
+  e->qstore.buf.release();
   e->qascii.release();
-  for (auto &s : e->slot) {
-    s.seeds.release();
-    s.cnt.release();
-    s.bst.release();
-  }
-  e->pairs.release();
-  e->pair_partial.release();
-  e->pair_total.release();
-  e->c_incl.release();
-  e->c_qpos.release();
-  e->c_bst.release();
-  e->bounds.release();
-  e->status.release();
-  e->raw_count.release();
-  e->bad.release();
-  e->anchors.release();
+  for (auto &s : e->slot) s.seeds.release();
+  e->calls.release();
+  e->pos_hits.release();
+  e->np_pos.release();
+  e->call_nz_lo.release();
+  e->scope_call.release();
+  e->raw_scope.release();
+  e->np_excl.release();
+  e->call_hit_lo.release();
+  e->scope_lo.release();
+  e->np_partial.release();
+  e->np_grand.release();
+  e->tot.release();
+  e->cand.release();
   e->raw.release();
-  e->cells.release();
-  e->n_valid.release();
-  e->h_stage.release();
+  e->h_calls.release();
+  e->h_tot.release();
   e->h_raw.release();
-  e->h_small.release();
+  e->h_raw_scope.release();
+  e->h_scope_call.release();
   for (auto &pe : e->pending) {
     cudaEventDestroy(pe.second.first);
     cudaEventDestroy(pe.second.second);
@@ -572,7 +723,7 @@ void hz_engine_destroy(hz_engine *e) {
 
 int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t index_len, const uint32_t *pos_table,
                           uint64_t pos_len, const uint8_t *ref_seq, uint64_t ref_len) {
-  if (!e || !index_table || !ref_seq || (pos_len && !pos_table)) return fail(HZ_E_INVALID, "null argument");
+  if (!e || !index_table || (ref_len && !ref_seq) || (pos_len && !pos_table)) return fail(HZ_E_INVALID, "null argument");
   if (index_len != (1ull << (2 * e->shape.kmer_size)))
     return fail(HZ_E_INVALID, "index_table has %llu entries, the seed needs 4^%u", (unsigned long long)index_len,
                 e->shape.kmer_size);
@@ -589,18 +740,20 @@ int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t in
     if ((uint64_t)pos_table[i] + e->shape.size > ref_len)
       return fail(HZ_E_INVALID, "pos_table[%llu]=%u leaves no full seed window in a %llu-base reference",
                   (unsigned long long)i, pos_table[i], (unsigned long long)ref_len);
+  for (uint64_t i = 0; i < ref_len; i++)
+    if (ref_seq[i] > 7) return fail(HZ_E_INVALID, "ref_seq[%llu]=%u is not a device-alphabet code", (unsigned long long)i, ref_seq[i]);
   TRY(set_device(e));
-  TRY(e->index_table.ensure(index_len, e->st));
-  TRY(e->pos_table.ensure(pos_len + 1, e->st));
-  TRY(e->ref.ensure(ref_len + 1, e->st));
-  CK(cudaMemcpyAsync(e->index_table.p, index_table, index_len * 4, cudaMemcpyHostToDevice, e->st));
-  if (pos_len) CK(cudaMemcpyAsync(e->pos_table.p, pos_table, pos_len * 4, cudaMemcpyHostToDevice, e->st));
-  CK(cudaMemcpyAsync(e->ref.p, ref_seq, ref_len, cudaMemcpyHostToDevice, e->st));
+  cudaStream_t s = e->st;
+  TRY(e->index_table.ensure(index_len, s));
+  TRY(e->pos_table.ensure(pos_len + 1, s));
+  TRY(e->ref.ensure(ref_len, s));
+  CK(cudaMemcpyAsync(e->index_table.p, index_table, index_len * 4, cudaMemcpyHostToDevice, s));
+  if (pos_len) CK(cudaMemcpyAsync(e->pos_table.p, pos_table, pos_len * 4, cudaMemcpyHostToDevice, s));
+  if (ref_len) CK(cudaMemcpyAsync(e->ref.base(), ref_seq, ref_len, cudaMemcpyHostToDevice, s));
   TRY(e->sync());
   e->index_len = index_len;
   e->n_pos = pos_len;
   e->rlen = (uint32_t)ref_len;
-  e->ep.rlen = e->rlen;
   e->has_target = true;
   return HZ_OK;
 }
@@ -620,12 +773,13 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   // ASCII -> device codes
   DBuf<uint8_t> ascii, junk;
   TRY(ascii.ensure(len + 1, st));
-  TRY(e->ref.ensure(len + 1, st));
+  TRY(e->ref.ensure(len, st));
   TRY(junk.ensure(len + 1, st));
-  CK(cudaMemcpyAsync(ascii.p, ref_ascii, len, cudaMemcpyHostToDevice, st));
+  if (len) CK(cudaMemcpyAsync(ascii.p, ref_ascii, len, cudaMemcpyHostToDevice, st));
+  uint8_t *codes = e->ref.base();
   if (len)
     TRY(e->launch("encode", [&] {
-      encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, st>>>(ascii.p, len, e->ref.p, junk.p);
+      encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, st>>>(ascii.p, len, codes, junk.p);
     }));
   TRY(e->index_table.ensure(index_len, st));
   CK(cudaMemsetAsync(e->index_table.p, 0, index_len * 4, st));
@@ -638,10 +792,10 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
     TRY(partial.ensure(scan_tiles(num_steps) + 1, st));
     TRY(total.ensure(1, st));
     TRY(e->launch("ref_kmer", [&] {
-      ref_kmer_kernel<<<grid_for(num_steps, 256), 256, 0, st>>>(e->ref.p, num_steps, start_offset, step, sh, kmers.p,
+      ref_kmer_kernel<<<grid_for(num_steps, 256), 256, 0, st>>>(codes, num_steps, start_offset, step, sh, kmers.p,
                                                                 flags.p);
     }));
-    TRY(e->launch("ref_scan", [&] { exclusive_scan<uint32_t>(flags.p, flags.p, num_steps, partial.p, total.p, st); }));
+    TRY(e->launch("ref_scan", [&] { exclusive_scan<uint32_t>(flags.p, flags.p, num_steps, partial.p, total.p, st); }, 3));
     uint32_t tot = 0;
     CK(cudaMemcpyAsync(&tot, total.p, 4, cudaMemcpyDeviceToHost, st));
     TRY(e->sync());
@@ -652,27 +806,26 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
       ref_compact_kernel<<<grid_for(num_steps, 256), 256, 0, st>>>(kmers.p, flags.p, num_steps, start_offset, step,
                                                                    keys.p, vals.p, e->index_table.p);
     }));
-    kmers.release();
-    flags.release();
-    // stable radix sort by k-mer, 8 bits per pass
+    // stable radix sort by k-mer, 8 bits per pass: each bucket keeps
+    // ascending position order (src/seed.rs:157-170)
     if (n_valid) {
       TRY(keys2.ensure(n_valid + 1, st));
       TRY(vals2.ensure(n_valid + 1, st));
-      uint64_t tiles = (n_valid + kRadixTile - 1) / kRadixTile;
-      TRY(hist.ensure(tiles * kRadixBins, st));
-      TRY(hpartial.ensure(scan_tiles(tiles * kRadixBins) + 1, st));
+      uint64_t rtiles = (n_valid + kRadixTile - 1) / kRadixTile;
+      TRY(hist.ensure(rtiles * kRadixBins, st));
+      TRY(hpartial.ensure(scan_tiles(rtiles * kRadixBins) + 1, st));
       int bits = 2 * (int)sh.kmer_size;
       uint32_t *ka = keys.p, *va = vals.p, *kb = keys2.p, *vb = vals2.p;
       for (int shift = 0; shift < bits; shift += 8) {
         TRY(e->launch("radix_hist", [&] {
-          radix_hist_kernel<<<(unsigned)tiles, kRadixThreads, 0, st>>>(ka, n_valid, shift, hist.p, tiles);
+          radix_hist_kernel<<<(unsigned)rtiles, kRadixThreads, 0, st>>>(ka, n_valid, shift, hist.p, rtiles);
         }));
         TRY(e->launch("radix_scan", [&] {
-          exclusive_scan<uint32_t>(hist.p, hist.p, tiles * kRadixBins, hpartial.p, total.p, st);
-        }));
+          exclusive_scan<uint32_t>(hist.p, hist.p, rtiles * kRadixBins, hpartial.p, total.p, st);
+        }, 3));
         TRY(e->launch("radix_scatter", [&] {
-          radix_scatter_kernel<<<(unsigned)tiles, kRadixThreads, 0, st>>>(ka, va, n_valid, shift, hist.p, tiles, kb,
-                                                                         vb);
+          radix_scatter_kernel<<<(unsigned)rtiles, kRadixThreads, 0, st>>>(ka, va, n_valid, shift, hist.p, rtiles, kb,
+                                                                          vb);
         }));
         std::swap(ka, kb);
         std::swap(va, vb);
@@ -682,7 +835,7 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
     }
   }
   TRY(e->pos_table.ensure(1, st));
-  // index_table = inclusive cumulative bucket counts
+  // index_table = inclusive cumulative bucket counts (src/seed.rs:162-164)
   {
     DBuf<uint32_t> excl, ipart;
     TRY(excl.ensure(index_len, st));
@@ -690,7 +843,7 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
     TRY(total.ensure(1, st));
     TRY(e->launch("index_scan", [&] {
       exclusive_scan<uint32_t>(e->index_table.p, excl.p, index_len, ipart.p, total.p, st);
-    }));
+    }, 3));
     TRY(e->launch("index_add", [&] {
       add_counts_kernel<<<grid_for(index_len, 256), 256, 0, st>>>(excl.p, e->index_table.p, index_len);
     }));
@@ -701,6 +854,8 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   }
   ascii.release();
   junk.release();
+  kmers.release();
+  flags.release();
   keys.release();
   vals.release();
   keys2.release();
@@ -712,7 +867,6 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   e->index_len = index_len;
   e->n_pos = n_valid;
   e->rlen = (uint32_t)len;
-  e->ep.rlen = e->rlen;
   e->has_target = true;
   return HZ_OK;
 }
@@ -732,13 +886,22 @@ int hz_engine_read_tables(hz_engine *e, uint32_t *index_table, uint64_t *index_l
 int hz_swap_query(hz_engine *e, const uint8_t *query, const uint8_t *query_rc, uint64_t len) {
   if (!e || (len && (!query || !query_rc))) return fail(HZ_E_INVALID, "null argument");
   if (len > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "query block exceeds u32 coordinates");
+  for (uint64_t i = 0; i < len; i++)
+    if (query[i] > 7 || query_rc[i] > 7) return fail(HZ_E_INVALID, "query byte %llu is not a device-alphabet code", (unsigned long long)i);
   TRY(set_device(e));
-  TRY(e->qf.ensure(len + 1, e->st));
-  TRY(e->qr.ensure(len + 1, e->st));
-  CK(cudaMemcpyAsync(e->qf.p, query, len, cudaMemcpyHostToDevice, e->st));
-  CK(cudaMemcpyAsync(e->qr.p, query_rc, len, cudaMemcpyHostToDevice, e->st));
+  StagedQuery q;
+  q.len = (uint32_t)len;
+  q.off_f = 0;
+  q.off_r = (uint32_t)((len + kPad + 15) & ~15ull);
+  uint64_t total = q.off_r + len + kPad;
+  TRY(e->qstore.ensure(total, e->st));
+  CK(cudaMemsetAsync(e->qstore.base(), 0, total, e->st));
+  if (len) {
+    CK(cudaMemcpyAsync(e->qstore.base() + q.off_f, query, len, cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemcpyAsync(e->qstore.base() + q.off_r, query_rc, len, cudaMemcpyHostToDevice, e->st));
+  }
   TRY(e->sync());
-  e->qlen = (uint32_t)len;
+  e->queries.assign(1, q);
   e->has_query = true;
   e->slot[0].kind = e->slot[1].kind = 0;
   return HZ_OK;
@@ -746,39 +909,34 @@ int hz_swap_query(hz_engine *e, const uint8_t *query, const uint8_t *query_rc, u
 
 int hz_swap_query_ascii(hz_engine *e, const uint8_t *q, uint64_t len) {
   if (!e || (len && !q)) return fail(HZ_E_INVALID, "null argument");
-  if (len > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "query block exceeds u32 coordinates");
   TRY(set_device(e));
-  TRY(e->qascii.ensure(len + 1, e->st));
-  TRY(e->qf.ensure(len + 1, e->st));
-  TRY(e->qr.ensure(len + 1, e->st));
-  CK(cudaMemcpyAsync(e->qascii.p, q, len, cudaMemcpyHostToDevice, e->st));
-  if (len)
-    TRY(e->launch("encode", [&] {
-      encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, e->st>>>(e->qascii.p, len, e->qf.p, e->qr.p);
-    }));
-  TRY(e->sync());
-  e->qlen = (uint32_t)len;
-  e->has_query = true;
-  e->slot[0].kind = e->slot[1].kind = 0;
-  return HZ_OK;
+  return stage_ascii(e, &q, &len, 1);
 }
 
 int hz_upload_seeds(hz_engine *e, uint32_t slot, const uint64_t *seeds, uint64_t n) {
   if (!e || slot > 1 || (n && !seeds)) return fail(HZ_E_INVALID, "bad argument");
+  if (!e->has_query) return fail(HZ_E_STATE, "Engine has no query: swap_query() must be called before upload_seeds()");
+  if (n >= 0x7FFFFFFFull) return fail(HZ_E_INVALID, "too many seeds in one call");
+  uint32_t qlen = e->queries[0].len;
+  uint32_t max_pos = qlen >= e->shape.size ? qlen - e->shape.size : 0;
+  for (uint64_t i = 0; i < n; i++) {
+    uint64_t k = seeds[i] >> 32;
+    if (k >= e->index_len || (uint32_t)seeds[i] > max_pos || qlen < e->shape.size)
+      return fail(HZ_E_INVALID, "seed %llu (k-mer %llu, position %u) lies outside the seed table or the query",
+                  (unsigned long long)i, (unsigned long long)k, (uint32_t)seeds[i]);
+  }
   TRY(set_device(e));
   Slot &s = e->slot[slot];
   TRY(s.seeds.ensure(n + 1, e->st));
   if (n) CK(cudaMemcpyAsync(s.seeds.p, seeds, n * 8, cudaMemcpyHostToDevice, e->st));
   TRY(e->sync());
   s.kind = 1;
-  s.n_slots = n;
-  s.n_seeds = n;
-  s.per_pos = 1;
-  s.start = 0;
-  s.counted = false;
+  s.n = n;
   return HZ_OK;
 }
 
+// Counts the valid windows of [start, end) so the seed count is known as
+// chunk_seeds would report it; the lookup itself runs in seed_and_filter.
 int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint32_t end, int transitions,
                       uint64_t *n_seeds) {
   if (!e || slot > 1) return fail(HZ_E_INVALID, "bad argument");
@@ -786,13 +944,47 @@ int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint
   if (!e->has_target) return fail(HZ_E_STATE, "no target loaded");
   TRY(check_range(e, start, end));
   TRY(set_device(e));
-  CK(cudaMemsetAsync(e->n_valid.p, 0, 8, e->st));
-  TRY(generate_into(e, e->slot[slot], rev, start, end, transitions));
-  unsigned long long nv = 0;
-  CK(cudaMemcpyAsync(&nv, e->n_valid.p, 8, cudaMemcpyDeviceToHost, e->st));
-  TRY(e->sync());
-  e->slot[slot].n_seeds = nv * e->slot[slot].per_pos;
-  if (n_seeds) *n_seeds = e->slot[slot].n_seeds;
+  Slot &s = e->slot[slot];
+  s.kind = 2;
+  s.rev = rev ? 1 : 0;
+  s.start = start;
+  s.end = end;
+  s.transitions = transitions ? 1 : 0;
+  uint64_t nv = 0;
+  if (end > start) {
+    // the lookup kernel counts valid windows as it goes: run it alone
+    const StagedQuery &q = e->queries[0];
+    TRY(e->h_calls.ensure(1));
+    e->h_calls.p[0] = CallDev{s.rev ? q.off_r : q.off_f, q.len, start, 0};
+    TRY(e->calls.ensure(1, e->st));
+    TRY(e->pos_hits.ensure(end - start, e->st));
+    TRY(e->tot.ensure(1, e->st));
+    TRY(e->h_tot.ensure(1));
+    CK(cudaMemcpyAsync(e->calls.p, e->h_calls.p, sizeof(CallDev), cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemsetAsync(e->tot.p, 0, sizeof(WaveTotals), e->st));
+    WaveIn w;
+    memset(&w, 0, sizeof w);
+    w.ref = e->ref.base();
+    w.rlen = e->rlen;
+    w.qbuf = e->qstore.base();
+    w.index_table = e->index_table.p;
+    w.pos_table = e->pos_table.p;
+    w.calls = e->calls.p;
+    w.ncalls = 1;
+    w.npos = end - start;
+    w.shape = e->shape;
+    w.per_pos = e->per_pos(transitions);
+    w.occ_cap = e->cfg.occ_cap;
+    TRY(e->launch("lookup_count", [&] {
+      lookup_count_kernel<<<(w.npos + kCountPerBlock - 1) / kCountPerBlock, kCountThreads, 0, e->st>>>(w, e->pos_hits.p,
+                                                                                                       e->tot.p);
+    }));
+    CK(cudaMemcpyAsync(e->h_tot.p, e->tot.p, sizeof(WaveTotals), cudaMemcpyDeviceToHost, e->st));
+    TRY(e->sync());
+    nv = e->h_tot.p->valid;
+  }
+  s.n = nv * e->per_pos(transitions);
+  if (n_seeds) *n_seeds = s.n;
   return HZ_OK;
 }
 
@@ -806,47 +998,25 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
   TRY(set_device(e));
   Slot &s = e->slot[slot];
   if (s.kind == 0) return fail(HZ_E_STATE, "seed slot %u holds no seeds", slot);
-  if (s.kind == 2 && s.rev != rev) return fail(HZ_E_INVALID, "slot %u was generated for the other strand", slot);
+  if (s.kind == 2 && s.rev != (rev ? 1 : 0)) return fail(HZ_E_INVALID, "slot %u was generated for the other strand", slot);
   hz_stats local;
   memset(&local, 0, sizeof local);
-  const uint8_t *q = rev ? e->qr.p : e->qf.p;
-  if (s.kind == 1 && !s.counted) {
-    TRY(s.cnt.ensure(s.n_slots + 1, e->st));
-    TRY(s.bst.ensure(s.n_slots + 1, e->st));
-    TRY(e->bad.ensure(1, e->st));
-    CK(cudaMemsetAsync(e->bad.p, 0, 4, e->st));
-    uint32_t max_pos = e->qlen >= e->shape.size ? e->qlen - e->shape.size : 0;
-    if (s.n_slots) {
-      uint64_t ns = s.n_slots;
-      TRY(e->launch("seed_count", [&] {
-        seed_count_uploaded_kernel<<<grid_for(ns, 256), 256, 0, e->st>>>(s.seeds.p, ns, e->index_table.p,
-                                                                         e->cfg.occ_cap, (uint32_t)e->index_len, max_pos,
-                                                                         s.cnt.p, s.bst.p, e->bad.p);
-      }));
-    }
-    uint32_t bad = 0;
-    CK(cudaMemcpyAsync(&bad, e->bad.p, 4, cudaMemcpyDeviceToHost, e->st));
-    TRY(e->sync());
-    if (bad) return fail(HZ_E_INVALID, "an uploaded seed has a k-mer or position outside the tables/query");
-    s.counted = true;
+  std::vector<WaveRecord> recs;
+  if (s.kind == 2) {
+    HostCall hc{0, 0, (uint32_t)(rev ? 1 : 0), s.start, s.end};
+    TRY(run_wave(e, &hc, s.end > s.start ? 1 : 0, nullptr, s.transitions, &recs, &local));
+  } else if (s.n) {
+    HostCall hc{0, 0, (uint32_t)(rev ? 1 : 0), 0, (uint32_t)s.n};
+    TRY(run_wave(e, &hc, 1, s.seeds.p, 0, &recs, &local));
   }
-  CK(cudaMemsetAsync(e->cells.p, 0, 8, e->st));
-  std::vector<hz_segment_pair> res;
-  TRY(filter_slot(e, s, q, res, &local));
-  unsigned long long cells = 0;
-  CK(cudaMemcpyAsync(&cells, e->cells.p, 8, cudaMemcpyDeviceToHost, e->st));
-  TRY(e->sync());
-  local.cells = cells;
-  if (!res.empty()) {
-    *out = (hz_segment_pair *)malloc(res.size() * sizeof(hz_segment_pair));
-    if (!*out) return fail(HZ_E_OOM, "host allocation");
-    memcpy(*out, res.data(), res.size() * sizeof(hz_segment_pair));
-  }
-  *n = res.size();
+  local.seeds = s.n;
+  TRY(copy_out_segments(recs, out, n));
   if (stats) *stats = local;
   return HZ_OK;
 }
 
+// The plain per-chunk form: one wave (launch chain + read-back + host dedup)
+// per seed_and_filter call, in the reference's call order.
 int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats) {
   if (!e || !out || !n) return fail(HZ_E_INVALID, "bad argument");
   *out = nullptr;
@@ -856,51 +1026,77 @@ int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats
   TRY(set_device(e));
   hz_stats local;
   memset(&local, 0, sizeof local);
-  uint32_t ss = e->shape.size;
-  uint64_t qlen = e->qlen;
-  // intervals (src/sequence.rs:322-334) and the batch list (src/run.rs:278-299)
-  std::vector<std::pair<uint32_t, uint32_t>> iv;
-  if (qlen > ss) {
-    uint32_t end_pos = (uint32_t)(qlen - ss);
-    for (uint64_t cur = 0; cur < end_pos; cur += e->cfg.interval)
-      iv.push_back({(uint32_t)cur, (uint32_t)std::min<uint64_t>(end_pos, cur + e->cfg.interval)});
+  std::vector<HostCall> calls;
+  query_calls(e, 0, &calls);
+  std::vector<WaveRecord> recs;
+  for (size_t i = 0; i < calls.size(); i++) {
+    size_t before = recs.size();
+    TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local));
+    for (size_t k = before; k < recs.size(); k++) recs[k].call = (uint32_t)i;  // wave-relative -> pass call
   }
-  uint32_t qbl = qlen > ss ? (uint32_t)(qlen - ss) : 0;
-  std::vector<hz_pass_record> recs;
-  CK(cudaMemsetAsync(e->cells.p, 0, 8, e->st));
-  CK(cudaMemsetAsync(e->n_valid.p, 0, 8, e->st));
-  Slot &s = e->slot[0];
-  for (size_t i = 0; i < iv.size(); i++) {
-    std::vector<hz_segment_pair> per[2];
-    for (int rev = 0; rev < 2; rev++) {
-      if (!(e->cfg.strand & (1u << rev))) continue;
-      uint32_t a = rev ? qbl - iv[i].second : iv[i].first;
-      uint32_t b = rev ? qbl - iv[i].first : iv[i].second;
-      for (uint64_t c = a; c < b; c += e->cfg.wga_chunk) {  // chunks(), src/seed.rs:488-496
-        uint32_t cs = (uint32_t)c, ce = (uint32_t)std::min<uint64_t>(c + e->cfg.wga_chunk, (uint64_t)b + 1);
-        TRY(generate_into(e, s, rev, cs, ce, e->cfg.transitions));
-        s.n_seeds = 0;
-        TRY(filter_slot(e, s, rev ? e->qr.p : e->qf.p, per[rev], &local));
-      }
-    }
-    for (int rev = 0; rev < 2; rev++)
-      for (auto &h : per[rev]) recs.push_back({(uint32_t)i, (uint32_t)rev, h});
-  }
-  unsigned long long cells = 0, nv = 0;
-  CK(cudaMemcpyAsync(&cells, e->cells.p, 8, cudaMemcpyDeviceToHost, e->st));
-  CK(cudaMemcpyAsync(&nv, e->n_valid.p, 8, cudaMemcpyDeviceToHost, e->st));
-  TRY(e->sync());
-  local.cells = cells;
-  local.seeds = nv * (e->cfg.transitions ? 1 + e->shape.kmer_size : 1);
-  // calls with no seeds are not calls in the reference (src/run.rs:431)
+  // records of one interval: plus calls before minus calls (call order already)
   if (!recs.empty()) {
     *out = (hz_pass_record *)malloc(recs.size() * sizeof(hz_pass_record));
     if (!*out) return fail(HZ_E_OOM, "host allocation");
-    memcpy(*out, recs.data(), recs.size() * sizeof(hz_pass_record));
+    for (size_t i = 0; i < recs.size(); i++)
+      (*out)[i] = hz_pass_record{calls[recs[i].call].interval, calls[recs[i].call].strand, recs[i].h};
   }
   *n = recs.size();
   if (stats) *stats = local;
   e->slot[0].kind = 0;
+  return HZ_OK;
+}
+
+int hz_stage_queries(hz_engine *e, const hz_query *queries, uint32_t nq) {
+  if (!e || (nq && !queries)) return fail(HZ_E_INVALID, "null argument");
+  std::vector<const uint8_t *> ptrs(nq);
+  std::vector<uint64_t> lens(nq);
+  for (uint32_t i = 0; i < nq; i++) {
+    if (queries[i].len && !queries[i].ascii) return fail(HZ_E_INVALID, "query %u has no bytes", i);
+    ptrs[i] = queries[i].ascii;
+    lens[i] = queries[i].len;
+  }
+  TRY(set_device(e));
+  return stage_ascii(e, ptrs.data(), lens.data(), nq);
+}
+
+// The batched form: the calls of all staged queries, query-major, cut into
+// waves of at most wave_positions seed positions at call boundaries.
+int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *stats) {
+  if (!e || !out || !n) return fail(HZ_E_INVALID, "bad argument");
+  *out = nullptr;
+  *n = 0;
+  if (!e->has_query) return fail(HZ_E_STATE, "no query staged");
+  if (!e->has_target) return fail(HZ_E_STATE, "no target loaded");
+  TRY(set_device(e));
+  hz_stats local;
+  memset(&local, 0, sizeof local);
+  std::vector<HostCall> calls;
+  for (uint32_t q = 0; q < e->queries.size(); q++) query_calls(e, q, &calls);
+  std::vector<WaveRecord> recs;
+  size_t i = 0;
+  while (i < calls.size()) {
+    size_t j = i;
+    uint64_t npos = 0;
+    while (j < calls.size() && (j == i || npos + (calls[j].end - calls[j].start) <= e->wave_positions)) {
+      npos += calls[j].end - calls[j].start;
+      j++;
+    }
+    size_t before = recs.size();
+    TRY(run_wave(e, calls.data() + i, j - i, nullptr, e->cfg.transitions, &recs, &local));
+    for (size_t k = before; k < recs.size(); k++) recs[k].call += (uint32_t)i;
+    i = j;
+  }
+  if (!recs.empty()) {
+    *out = (hz_batch_record *)malloc(recs.size() * sizeof(hz_batch_record));
+    if (!*out) return fail(HZ_E_OOM, "host allocation");
+    for (size_t k = 0; k < recs.size(); k++) {
+      const HostCall &c = calls[recs[k].call];
+      (*out)[k] = hz_batch_record{c.query, c.interval, c.strand, recs[k].h};
+    }
+  }
+  *n = recs.size();
+  if (stats) *stats = local;
   return HZ_OK;
 }
 
@@ -940,6 +1136,27 @@ int hz_engine_profile_reset(hz_engine *e) {
 }
 
 uint64_t hz_engine_launches(hz_engine *e) { return e ? e->launches : 0; }
+
+int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
+  if (!e || !key) return fail(HZ_E_INVALID, "null argument");
+  std::string k(key);
+  if (k == "gate_tile") {
+    if (value != 1024 && value != 2048 && value != 4096) return fail(HZ_E_INVALID, "gate_tile must be 1024, 2048 or 4096");
+    e->gate_tile = (int)value;
+  } else if (k == "gate_cap") {
+    if (value < 8 || value > 65528 || value % 8) return fail(HZ_E_INVALID, "gate_cap must be a multiple of 8 in 8..65528");
+    e->gate_cap = (uint32_t)value;
+  } else if (k == "gate_blocks_per_sm") {
+    if (value < 0 || value > 32) return fail(HZ_E_INVALID, "gate_blocks_per_sm must be 0..32");
+    e->gate_blocks_per_sm = (int)value;
+  } else if (k == "wave_positions") {
+    if (value < 1 || value >= (1ll << 31)) return fail(HZ_E_INVALID, "wave_positions must be 1..2^31-1");
+    e->wave_positions = (uint64_t)value;
+  } else {
+    return fail(HZ_E_INVALID, "unknown tuning key %s", key);
+  }
+  return HZ_OK;
+}
 
 int hz_engine_set_stream(hz_engine *e, void *stream) {
   if (!e) return fail(HZ_E_INVALID, "null engine");

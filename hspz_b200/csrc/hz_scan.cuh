@@ -27,6 +27,19 @@ template <> struct Sum<uint2> {
   }
 };
 
+// A 64-bit hit count paired with a 32-bit position count.
+struct HitNz {
+  unsigned long long h;
+  uint32_t n;
+};
+template <> struct Sum<HitNz> {
+  __device__ __forceinline__ static HitNz zero() { return HitNz{0ull, 0u}; }
+  __device__ __forceinline__ static HitNz add(HitNz a, HitNz b) { return HitNz{a.h + b.h, a.n + b.n}; }
+  __device__ __forceinline__ static HitNz shfl_up(HitNz v, int d) {
+    return HitNz{__shfl_up_sync(0xffffffffu, v.h, d), __shfl_up_sync(0xffffffffu, v.n, d)};
+  }
+};
+
 // Exclusive block scan of one value per thread; returns the exclusive prefix
 // and writes the block total to *total.
 template <typename T>

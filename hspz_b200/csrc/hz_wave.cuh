@@ -1,0 +1,821 @@
+// The wave pipeline: any number of seed_and_filter calls (one WGA chunk of
+// one strand of one query each) processed by one fixed sequence of launches.
+//
+//   lookup_count   per query position: the capped hit counts of its seeds
+//   np_*           scan of the counts; compaction of positions with hits
+//   scopes         per call: hit range and MAX_HITS dedup scopes
+//   gate           fused hit expansion + thread-per-hit X-drop score gate
+//   exact          warp-per-candidate X-drop with positions, entropy, accept
+//
+// Semantics follow hspZ src/gpu/kernels.rs and src/gpu/mod.rs (cited per
+// kernel).  Hit indices are 64-bit across a wave (a call's own hit count is
+// a u32, as in the reference).  Sizes that depend on the data (hits,
+// candidates, HSPs) are read from device memory, so a wave needs no host
+// round trip until its output.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hz_device.cuh"
+#include "hz_scan.cuh"
+
+namespace hz {
+
+// One seed_and_filter call of a wave.
+struct CallDev {
+  uint32_t qoff;     // offset of the strand block's position 0 in the query store
+  uint32_t qlen;     // block length (right edge of the extension)
+  uint32_t start;    // first seed position of the call (block coordinates)
+  uint32_t pos_off;  // first flat position of the call in the wave
+};
+
+// Inputs shared by the lookup, scope and gate kernels.
+struct WaveIn {
+  const uint8_t *ref;  // reference codes (padded on both sides)
+  uint32_t rlen;
+  const uint8_t *qbuf;  // query store (padded)
+  const uint32_t *index_table;
+  const uint32_t *pos_table;
+  const CallDev *calls;
+  uint32_t ncalls;
+  uint32_t npos;          // flat positions of the wave
+  const uint64_t *seeds;  // host-uploaded seeds (one per flat position) or null
+  ShapeDev shape;
+  uint32_t per_pos;  // seeds per position: 1 + kmer_size with transitions, else 1
+  uint32_t occ_cap;
+};
+
+// Device-side counters of a wave.
+struct WaveTotals {
+  unsigned long long hits;   // seed hits of the wave
+  unsigned long long cells;  // scalar X-drop cells scored
+  unsigned long long valid;  // valid seed windows
+  unsigned long long tiles;  // gate work-queue cursor
+  uint32_t nz;               // positions with at least one hit
+  uint32_t n_scopes;
+  uint32_t status;  // bit 0: a call's first seed alone exceeds max_hits; bit 1: a call exceeds 2^32 hits
+  uint32_t cand;    // gate candidates written (may exceed capacity)
+  uint32_t raw;     // accepted HSPs written (may exceed capacity)
+  uint32_t pad[3];
+};
+
+// Gate candidate: a hit whose score bound passes the threshold, or whose
+// extension ran past the per-direction cap ("long").
+struct Cand {
+  uint32_t scope;  // dedup scope of the hit
+  uint32_t r0;     // reference anchor
+  uint32_t q0;     // query anchor, absolute in the query store
+  uint32_t call;   // call index | kLongFlag
+};
+constexpr uint32_t kLongFlag = 1u << 31;
+
+__device__ __forceinline__ uint32_t call_of(const CallDev *calls, uint32_t ncalls, uint32_t p) {
+  uint32_t lo = 0, hi = ncalls;  // last call with pos_off <= p
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (calls[mid].pos_off <= p) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Seed of flat position p: (query position, k-mer); false for an invalid
+// window.  src/seed.rs:88-123.
+__device__ __forceinline__ bool position_seed(const WaveIn &w, const CallDev &c, uint32_t p, uint32_t *qpos,
+                                              uint32_t *kmer) {
+  if (w.seeds) {
+    uint64_t s = w.seeds[p];
+    *kmer = (uint32_t)(s >> 32);
+    *qpos = (uint32_t)s;
+    return true;
+  }
+  *qpos = c.start + (p - c.pos_off);
+  *kmer = kmer_at(w.qbuf + c.qoff, *qpos, w.shape);
+  return *kmer != kInvalidKmer;
+}
+
+// Seed v of a position: the exact k-mer, then kmer ^ (2 << 2(v-1))
+// (push_seeds, src/seed.rs:107-123).
+__device__ __forceinline__ uint32_t seed_variant(uint32_t kmer, uint32_t v) {
+  return v == 0 ? kmer : kmer ^ (2u << (2 * (v - 1)));
+}
+
+// find_num_hits with the occurrence cap (src/gpu/kernels.rs:70-115).
+__device__ __forceinline__ uint32_t bucket(const WaveIn &w, uint32_t k, uint32_t *beg) {
+  uint32_t end = __ldg(w.index_table + k);
+  uint32_t b = k ? __ldg(w.index_table + k - 1) : 0u;
+  uint32_t c = end - b;
+  if (w.occ_cap && c > w.occ_cap) c = 0;
+  *beg = b;
+  return c;
+}
+
+// last index in [lo, hi) whose value is <= h (caller guarantees one exists)
+__device__ __forceinline__ uint32_t last_le(const unsigned long long *v, uint32_t lo, uint32_t hi,
+                                            unsigned long long h) {
+  uint32_t a = lo, b = hi;  // first index with v > h
+  while (a < b) {
+    uint32_t m = (a + b) >> 1;
+    if (v[m] <= h) a = m + 1; else b = m;
+  }
+  return a - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Per flat position: total hits of its seeds.
+constexpr int kCountThreads = 256;
+constexpr int kCountPerBlock = 1024;
+
+__global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, uint32_t *__restrict__ pos_hits,
+                                                                     WaveTotals *__restrict__ tot) {
+  __shared__ uint32_t s_c0;
+  uint32_t p0 = blockIdx.x * kCountPerBlock;
+  if (threadIdx.x == 0) s_c0 = call_of(w.calls, w.ncalls, p0);
+  __syncthreads();
+  uint32_t c = s_c0;
+  uint32_t valid = 0;
+#pragma unroll 1
+  for (int i = 0; i < kCountPerBlock / kCountThreads; i++) {
+    uint32_t p = p0 + i * kCountThreads + threadIdx.x;
+    if (p >= w.npos) break;
+    while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+    CallDev cd = w.calls[c];
+    uint32_t qpos, kmer, sum = 0;
+    if (position_seed(w, cd, p, &qpos, &kmer)) {
+      valid++;
+      for (uint32_t v = 0; v < w.per_pos; v++) {
+        uint32_t beg;
+        sum += bucket(w, seed_variant(kmer, v), &beg);
+      }
+    }
+    pos_hits[p] = sum;
+  }
+  for (int d = 16; d > 0; d >>= 1) valid += __shfl_down_sync(0xffffffffu, valid, d);
+  if ((threadIdx.x & 31) == 0 && valid) atomicAdd(&tot->valid, (unsigned long long)valid);
+}
+
+// Scan of (hits, has-hits) over positions, then compaction of the positions
+// with hits: np_excl = hits of the wave before the position, np_pos = its
+// flat index.
+__global__ void __launch_bounds__(kScanThreads) np_reduce_kernel(const uint32_t *__restrict__ pos_hits, uint64_t n,
+                                                                 HitNz *__restrict__ partial) {
+  uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  HitNz acc = HitNz{0ull, 0u};
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++)
+    if (base + i < n) {
+      uint32_t h = pos_hits[base + i];
+      acc.h += h;
+      acc.n += h > 0;
+    }
+  HitNz tot;
+  block_exclusive_scan<HitNz>(acc, &tot);
+  if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *__restrict__ pos_hits, uint64_t n,
+                                                               const HitNz *__restrict__ partial,
+                                                               unsigned long long *__restrict__ np_excl,
+                                                               uint32_t *__restrict__ np_pos) {
+  uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  HitNz acc = HitNz{0ull, 0u};
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    v[i] = base + i < n ? pos_hits[base + i] : 0u;
+    acc.h += v[i];
+    acc.n += v[i] > 0;
+  }
+  HitNz tot;
+  HitNz ex = block_exclusive_scan<HitNz>(acc, &tot);
+  HitNz off = partial[blockIdx.x];
+  ex.h += off.h;
+  ex.n += off.n;
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    if (v[i]) {
+      np_excl[ex.n] = ex.h;
+      np_pos[ex.n] = (uint32_t)(base + i);
+      ex.h += v[i];
+      ex.n += 1;
+    }
+  }
+}
+
+// Grand totals of the scan into WaveTotals, and the sentinel np_excl[nz].
+__global__ void np_totals_kernel(const HitNz *__restrict__ grand, WaveTotals *__restrict__ t,
+                                 unsigned long long *__restrict__ np_excl) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    t->hits = grand->h;
+    t->nz = grand->n;
+    np_excl[grand->n] = grand->h;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per call: hit range, and the MAX_HITS dedup scopes (chunk_limits,
+// src/gpu/mod.rs:2394-2420, and the single-chunk shortcut when num_hits <=
+// max_hits, :1693-1705).  One block; calls are processed in rounds of
+// blockDim with a running scope offset, so scopes come out in call order and
+// tile the wave's hit space: scope s is [scope_lo[s], scope_lo[s+1]).  A cut
+// is the largest cumulative seed hit count below the running limit; it is
+// found over the positions with hits and refined by recounting the seeds of
+// the position the cut falls in (positions without hits repeat the
+// cumulative value before them, so they never move a cut).
+constexpr int kScopeThreads = 1024;
+
+__global__ void __launch_bounds__(kScopeThreads) scopes_kernel(WaveIn w, const unsigned long long *__restrict__ np_excl,
+                                                               const uint32_t *__restrict__ np_pos,
+                                                               WaveTotals *__restrict__ tot, uint32_t max_hits,
+                                                               unsigned long long *__restrict__ call_hit_lo,
+                                                               uint32_t *__restrict__ call_nz_lo,
+                                                               unsigned long long *__restrict__ scope_lo,
+                                                               uint32_t *__restrict__ scope_call, uint32_t scope_cap) {
+  __shared__ uint32_t s_w[32];
+  __shared__ uint32_t s_carry;
+  const unsigned long long total = tot->hits;
+  const uint32_t nz = tot->nz;
+  for (uint32_t c = threadIdx.x; c <= w.ncalls; c += blockDim.x) {
+    uint32_t k = nz;
+    if (c < w.ncalls) {
+      uint32_t p = w.calls[c].pos_off;
+      uint32_t a = 0, b = nz;  // first position with hits at or after the call start
+      while (a < b) {
+        uint32_t m = (a + b) >> 1;
+        if (np_pos[m] < p) a = m + 1; else b = m;
+      }
+      k = a;
+    }
+    call_nz_lo[c] = k;
+    call_hit_lo[c] = k < nz ? np_excl[k] : total;
+  }
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (uint32_t r0 = 0; r0 < w.ncalls; r0 += blockDim.x) {
+    uint32_t c = r0 + threadIdx.x;
+    uint32_t nsc = 0;
+    unsigned long long lo = 0, nh = 0;
+    if (c < w.ncalls) {
+      lo = call_hit_lo[c];
+      nh = call_hit_lo[c + 1] - lo;
+      if (nh > 0xFFFFFFFFull) {
+        atomicOr(&tot->status, 2u);
+        nh = 0;
+      }
+      nsc = nh <= max_hits ? 1u : (uint32_t)(nh / max_hits) + 1u;
+    }
+    uint32_t incl = nsc;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += up;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t xi = s_w[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t up = __shfl_up_sync(0xffffffffu, xi, d);
+        if (lane >= d) xi += up;
+      }
+      s_w[lane] = xi;
+    }
+    __syncthreads();
+    uint32_t s0 = s_carry + (wid ? s_w[wid - 1] : 0u) + incl - nsc;
+    uint32_t round_total = s_w[31];
+    if (c < w.ncalls && s0 + nsc <= scope_cap) {
+      scope_lo[s0] = lo;
+      scope_call[s0] = c;
+      if (nsc > 1) {
+        // the first real seed: the reference's walk has no cut when it
+        // alone holds >= max_hits hits (lower_bound - 1 underflows)
+        CallDev cd = w.calls[c];
+        uint32_t span = c + 1 < w.ncalls ? w.calls[c + 1].pos_off - cd.pos_off : w.npos - cd.pos_off;
+        for (uint32_t i = 0; i < span; i++) {
+          uint32_t qpos, kmer;
+          if (position_seed(w, cd, cd.pos_off + i, &qpos, &kmer)) {
+            uint32_t beg;
+            if (bucket(w, kmer, &beg) >= max_hits) atomicOr(&tot->status, 1u);
+            break;
+          }
+        }
+        uint32_t klo = call_nz_lo[c], khi = call_nz_lo[c + 1];
+        uint32_t limit = max_hits;  // relative to lo
+        for (uint32_t it = 1; it < nsc; it++) {
+          // last position of the call whose first hit is below the limit
+          uint32_t a = klo, b = khi;
+          while (a < b) {
+            uint32_t m = (a + b) >> 1;
+            if (np_excl[m] - lo < limit) a = m + 1; else b = m;
+          }
+          uint32_t B = 0;
+          if (a > klo) {
+            uint32_t k = a - 1;
+            uint32_t e = (uint32_t)(np_excl[k] - lo);
+            B = e;
+            uint32_t p = np_pos[k];
+            CallDev pc = w.calls[call_of(w.calls, w.ncalls, p)];
+            uint32_t qpos, kmer;
+            position_seed(w, pc, p, &qpos, &kmer);
+            uint32_t run = e;
+            for (uint32_t v = 0; v < w.per_pos; v++) {
+              uint32_t beg;
+              run += bucket(w, seed_variant(kmer, v), &beg);
+              if (run < limit) B = run; else break;
+            }
+          }
+          scope_lo[s0 + it] = lo + B;
+          scope_call[s0 + it] = c;
+          limit = B + max_hits;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += round_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    tot->n_scopes = s_carry;
+    if (s_carry < scope_cap) scope_lo[s_carry] = total;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gate: a persistent grid takes tiles of consecutive wave hits from a device
+// work queue.  Per tile it (1) recomputes the seeds of the positions
+// covering the tile and records the (position, seed) slots overlapping it,
+// (2) gives every hit its slot by a block max-scan of slot-start marks and
+// gathers its reference anchor from pos_table (coalesced within a slot), then
+// (3) runs the X-drop score gate thread-per-hit, all right extensions first
+// and all left extensions second, each lane refilling from the tile when its
+// extension ends, so extensions of different length do not idle the warp.
+// Eight cells are scored per step from two 4-byte words of each sequence.
+// Anchors are the END of the seed window on both sides (pos + seed_size,
+// src/gpu/kernels.rs:397-401).  A hit becomes a candidate when
+// (i32)(f32)(right max + left max) >= hspthresh -- the reference gate's bound
+// (src/gpu/kernels.rs:1048-1052), never below the final score since the
+// entropy factor is <= 1 -- or when an extension runs past `cap` cells
+// ("long"; the exact kernel redoes it warp-wide).
+
+// Slot records sit at the tile-relative index of their first hit, so a
+// max-scan of "first hit + 1" marks gives every hit its slot.
+template <int TILE>
+struct GateSmem {
+  int32_t sub[64];
+  uint32_t slot_bst[TILE];    // pos_table index of the slot's first in-tile hit
+  uint32_t slot_q[TILE];      // query anchor (absolute)
+  uint32_t slot_call[TILE];
+  uint32_t hit_slot[TILE];    // first hit of the hit's slot + 1 (mark, then max-scan)
+  uint32_t hit_r[TILE];       // reference anchor of each hit
+  int32_t hit_rmax[TILE];     // right-extension maximum, or kSpilled
+  uint16_t hit_rcells[TILE];  // right-extension cells (<= cap)
+  uint32_t warp_tot[kScanThreads / 32];
+  unsigned long long h0;
+  uint32_t next, e0, e1;
+};
+constexpr int32_t kSpilled = -1;  // a right maximum is never negative
+
+struct GateArgs {
+  WaveIn w;
+  const unsigned long long *np_excl;
+  const uint32_t *np_pos;
+  const unsigned long long *scope_lo;
+  uint32_t scope_cap;  // entries of scope_lo (a wave with more scopes is rerun)
+  WaveTotals *tot;
+  int32_t sub[64];
+  int32_t xdrop;
+  int32_t hspthresh;
+  uint32_t cap;  // cells per direction before a hit goes to the exact kernel (multiple of 8)
+  Cand *cand;
+  uint32_t cand_cap;
+};
+
+__device__ __forceinline__ const uint32_t *word_ptr(const uint8_t *p) {
+  return reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)3);
+}
+
+// Inclusive max-scan of the slot marks over the tile.
+template <int TILE>
+__device__ __forceinline__ void mark_scan(GateSmem<TILE> &sm, uint32_t nt) {
+  constexpr int PER = TILE / kScanThreads;
+  uint32_t base = threadIdx.x * PER;
+  uint32_t run = 0;
+#pragma unroll
+  for (int i = 0; i < PER; i++)
+    if (base + i < nt) run = max(run, sm.hit_slot[base + i]);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t incl = run;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl = max(incl, up);
+  }
+  if (lane == 31) sm.warp_tot[wid] = incl;
+  __syncthreads();
+  uint32_t carry = 0;
+  for (int i = 0; i < wid; i++) carry = max(carry, sm.warp_tot[i]);
+  uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane > 0) carry = max(carry, ex);
+#pragma unroll
+  for (int i = 0; i < PER; i++)
+    if (base + i < nt) {
+      carry = max(carry, sm.hit_slot[base + i]);
+      sm.hit_slot[base + i] = carry;
+    }
+}
+
+__device__ __forceinline__ uint32_t scope_of(const unsigned long long *scope_lo, uint32_t nscopes,
+                                             unsigned long long h) {
+  uint32_t lo = 0, hi = nscopes;  // last scope with scope_lo <= h
+  while (hi - lo > 1) {
+    uint32_t m = (lo + hi) >> 1;
+    if (scope_lo[m] <= h) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+// Scores one cell whose byte offset into the substitution table is byte SH
+// of T; keeps every running sum S and maximum M for the termination path.
+#define HZ_CELL(T, SH, I)                                                            \
+  {                                                                                  \
+    int32_t sc = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH)) & 0xFFu)); \
+    S = (int32_t)((uint32_t)S + (uint32_t)sc);                                       \
+    M = max(M, S);                                                                   \
+    Si[I] = S;                                                                       \
+    Mi[I] = M;                                                                       \
+    D = max(D, (int32_t)((uint32_t)M - (uint32_t)S));                                \
+  }
+
+template <int TILE, bool LEFT>
+__device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm, uint32_t nt,
+                                           unsigned long long &cells_acc) {
+  const uint8_t *ref = a.w.ref;
+  const uint8_t *qbuf = a.w.qbuf;
+  const char *subb = reinterpret_cast<const char *>(sm.sub);
+  const int32_t X = a.xdrop;
+  const uint32_t lane = threadIdx.x & 31;
+  bool have = false, exhausted = false;
+  uint32_t t = 0, n = 0, r0 = 0, q0 = 0;
+  bool capped = false;
+  int32_t S = 0, M = 0;
+  uint32_t cells = 0;
+  const uint32_t *wr = nullptr, *wq = nullptr;
+  uint32_t cr = 0, cq = 0, sr = 0, sq = 0;
+  while (true) {
+    if (!exhausted) {
+      unsigned need = __ballot_sync(0xffffffffu, !have);
+      if (need) {
+        int leader = __ffs(need) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(&sm.next, (uint32_t)__popc(need));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (base + __popc(need) >= nt) exhausted = true;
+        if (!have) {
+          uint32_t mine = base + __popc(need & lanemask_lt());
+          if (mine < nt && !(LEFT && sm.hit_rmax[mine] == kSpilled)) {
+            have = true;
+            t = mine;
+            uint32_t slot = sm.hit_slot[t] - 1;
+            r0 = sm.hit_r[t];
+            q0 = sm.slot_q[slot];
+            const CallDev &cd = a.w.calls[sm.slot_call[slot]];
+            uint32_t qlo = cd.qoff;
+            if (!LEFT) n = min(a.w.rlen - r0, qlo + cd.qlen - q0);
+            else n = min(r0, q0 - qlo);
+            capped = n > a.cap;
+            if (capped) n = a.cap;
+            S = 0;
+            M = 0;
+            cells = 0;
+            sr = (r0 & 3u) * 8u;
+            sq = (q0 & 3u) * 8u;
+            if (!LEFT) {
+              wr = word_ptr(ref + r0);
+              wq = word_ptr(qbuf + q0);
+              cr = __ldg(wr);
+              cq = __ldg(wq);
+            } else {
+              wr = word_ptr(ref + r0 - 8);
+              wq = word_ptr(qbuf + q0 - 8);
+              cr = __ldg(wr + 2);
+              cq = __ldg(wq + 2);
+            }
+          }
+        }
+      }
+    }
+    // (in the left pass a refill may hand out only hits that were spilled in
+    // the right pass, so an idle warp ends only once the tile is exhausted)
+    if (!__any_sync(0xffffffffu, have) && exhausted) break;
+    if (!have) continue;
+    // ---- eight cells ----
+    uint32_t ra, rb, qa, qb;
+    if (!LEFT) {
+      uint32_t rm = __ldg(wr + 1), rh = __ldg(wr + 2);
+      uint32_t qm = __ldg(wq + 1), qh = __ldg(wq + 2);
+      ra = __funnelshift_r(cr, rm, sr);
+      rb = __funnelshift_r(rm, rh, sr);
+      qa = __funnelshift_r(cq, qm, sq);
+      qb = __funnelshift_r(qm, qh, sq);
+      cr = rh;
+      cq = qh;
+      wr += 2;
+      wq += 2;
+    } else {
+      uint32_t rm = __ldg(wr + 1), rl = __ldg(wr);
+      uint32_t qm = __ldg(wq + 1), ql = __ldg(wq);
+      ra = __byte_perm(__funnelshift_r(rm, cr, sr), 0, 0x0123);
+      rb = __byte_perm(__funnelshift_r(rl, rm, sr), 0, 0x0123);
+      qa = __byte_perm(__funnelshift_r(qm, cq, sq), 0, 0x0123);
+      qb = __byte_perm(__funnelshift_r(ql, qm, sq), 0, 0x0123);
+      cr = rl;
+      cq = ql;
+      wr -= 2;
+      wq -= 2;
+    }
+    // codes are 0..7, so (r << 5) | (q << 2) is the byte offset of sub[r*8+q]
+    uint32_t ta = (ra << 5) | (qa << 2), tb = (rb << 5) | (qb << 2);
+    const int32_t Ms = M;
+    int32_t Si[8], Mi[8];
+    int32_t D = 0;
+    HZ_CELL(ta, 0, 0)
+    HZ_CELL(ta, 8, 1)
+    HZ_CELL(ta, 16, 2)
+    HZ_CELL(ta, 24, 3)
+    HZ_CELL(tb, 0, 4)
+    HZ_CELL(tb, 8, 5)
+    HZ_CELL(tb, 16, 6)
+    HZ_CELL(tb, 24, 7)
+    if (D <= X && n > 8) {  // no drop and more cells left
+      n -= 8;
+      cells += 8;
+      continue;
+    }
+    // The extension ends in this group: at the first valid cell with
+    // M - S > xdrop (keeping the maximum from before it), or after the v
+    // valid cells left before the edge or the cap.
+    uint32_t v = min(n, 8u);
+    uint32_t dm = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
+    dm &= (1u << v) - 1u;
+    uint32_t stop = dm ? (uint32_t)(__ffs(dm) - 1) : v;
+    int32_t res = Ms;
+#pragma unroll
+    for (int i = 1; i <= 8; i++)
+      if ((uint32_t)i == stop) res = Mi[i - 1];
+    cells += dm ? stop + 1 : v;
+    const bool spill = !dm && capped;
+    if (spill) {
+      uint32_t at = atomicAdd(&a.tot->cand, 1u);
+      if (at < a.cand_cap) {
+        uint32_t slot = sm.hit_slot[t] - 1;
+        a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), r0, q0,
+                             sm.slot_call[slot] | kLongFlag};
+      }
+      if (!LEFT) sm.hit_rmax[t] = kSpilled;  // the left pass skips it
+    } else if (!LEFT) {
+      sm.hit_rmax[t] = res;
+      sm.hit_rcells[t] = (uint16_t)cells;
+    } else {
+      cells_acc += cells + sm.hit_rcells[t];
+      int32_t total = (int32_t)((uint32_t)sm.hit_rmax[t] + (uint32_t)res);
+      if (sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
+        uint32_t at = atomicAdd(&a.tot->cand, 1u);
+        if (at < a.cand_cap) {
+          uint32_t slot = sm.hit_slot[t] - 1;
+          a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), r0, q0,
+                             sm.slot_call[slot]};
+        }
+      }
+    }
+    have = false;
+  }
+}
+
+template <int TILE>
+__global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
+  static_assert(TILE % kScanThreads == 0, "tile must be a multiple of the block");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GateSmem<TILE> &sm = *reinterpret_cast<GateSmem<TILE> *>(smem_raw);
+  if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
+  unsigned long long cells_acc = 0;
+  const unsigned long long total = a.tot->hits;
+  const uint32_t nz = a.tot->nz;
+  const WaveIn &w = a.w;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) sm.h0 = atomicAdd(&a.tot->tiles, 1ull) * (unsigned long long)TILE;
+    __syncthreads();
+    const unsigned long long h0 = sm.h0;
+    if (h0 >= total) break;
+    const uint32_t nt = (uint32_t)min((unsigned long long)TILE, total - h0);
+    // positions covering [h0, h0 + nt)
+    if (threadIdx.x < 2) {
+      unsigned long long h = threadIdx.x == 0 ? h0 : h0 + nt - 1;
+      uint32_t k = last_le(a.np_excl, 0, nz, h);
+      if (threadIdx.x == 0) sm.e0 = k; else sm.e1 = k;
+    }
+    if (threadIdx.x == 0) sm.next = 0;
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) sm.hit_slot[i] = 0;
+    __syncthreads();
+    // (1) slots overlapping the tile
+    const uint32_t e0 = sm.e0, e1 = sm.e1;
+    for (uint32_t k = e0 + threadIdx.x; k <= e1; k += blockDim.x) {
+      uint32_t p = a.np_pos[k];
+      uint32_t c = call_of(w.calls, w.ncalls, p);
+      CallDev cd = w.calls[c];
+      uint32_t qpos, kmer;
+      position_seed(w, cd, p, &qpos, &kmer);
+      unsigned long long lo = a.np_excl[k];
+      for (uint32_t v = 0; v < w.per_pos; v++) {
+        uint32_t beg;
+        uint32_t cnt = bucket(w, seed_variant(kmer, v), &beg);
+        unsigned long long hi = lo + cnt;
+        if (cnt && hi > h0 && lo < h0 + nt) {
+          unsigned long long first = lo > h0 ? lo : h0;
+          uint32_t s = (uint32_t)(first - h0);
+          sm.slot_bst[s] = beg + (uint32_t)(first - lo);
+          sm.slot_q[s] = cd.qoff + qpos + w.shape.size;
+          sm.slot_call[s] = c;
+          sm.hit_slot[s] = s + 1;
+        }
+        lo = hi;
+      }
+    }
+    __syncthreads();
+    // (2) hit -> slot, reference anchor
+    mark_scan<TILE>(sm, nt);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+      uint32_t s = sm.hit_slot[i] - 1;
+      sm.hit_r[i] = __ldg(w.pos_table + sm.slot_bst[s] + (i - s)) + w.shape.size;
+    }
+    __syncthreads();
+    // (3) the score gate
+    gate_phase<TILE, false>(a, sm, nt, cells_acc);
+    __syncthreads();
+    if (threadIdx.x == 0) sm.next = 0;
+    __syncthreads();
+    gate_phase<TILE, true>(a, sm, nt, cells_acc);
+  }
+  for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
+  if ((threadIdx.x & 31) == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
+}
+
+// ---------------------------------------------------------------------------
+// Exact extension, one warp per candidate: the reference's warp mapping of
+// find_hsps (src/gpu/kernels.rs:1279-1543) -- 32 cells per step, inclusive
+// sum and max scans, the first dropping lane by ballot, earliest-lane ties --
+// then the entropy correction and final threshold (:1555-1701).
+
+struct ExactArgs {
+  const uint8_t *ref;
+  uint32_t rlen;
+  const uint8_t *qbuf;
+  const CallDev *calls;
+  const Cand *cand;
+  uint32_t cand_cap;
+  WaveTotals *tot;
+  int32_t sub[64];
+  int32_t xdrop;
+  int32_t hspthresh;
+  uint32_t noentropy;
+  SegmentPair *raw;
+  uint32_t *raw_scope;
+  uint32_t raw_cap;
+};
+
+__device__ __forceinline__ int32_t warp_incl_sum(int32_t v, uint32_t lane) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int32_t up = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= (uint32_t)d) v = (int32_t)((uint32_t)v + (uint32_t)up);
+  }
+  return v;
+}
+
+// shuffle-up hands lanes below the offset their own value, so max(v, v) is a no-op
+__device__ __forceinline__ int32_t warp_incl_max(int32_t v) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int32_t up = __shfl_up_sync(0xffffffffu, v, d);
+    if (up >= v) v = up;
+  }
+  return v;
+}
+
+// One direction; returns (max, position) and adds the scored cells.
+template <bool LEFT>
+__device__ __forceinline__ void exact_dir(const uint8_t *ref, const uint8_t *qry, const int32_t *sub, int32_t X,
+                                          uint32_t r0, uint32_t q0, uint32_t nmax, uint32_t lane, int32_t *out_max,
+                                          int32_t *out_pos, unsigned long long *cells) {
+  int32_t prev_s = 0, prev_m = 0, prev_pos = LEFT ? 0 : -1;
+  for (uint32_t tile = 0;; tile += 32) {
+    uint32_t k = tile + lane;
+    int32_t sc = 0;
+    if (k < nmax) {
+      uint32_t rc = LEFT ? ref[r0 - 1 - k] : ref[r0 + k];
+      uint32_t qc = LEFT ? qry[q0 - 1 - k] : qry[q0 + k];
+      sc = sub[rc * kNuc + qc];
+    }
+    int32_t ts = (int32_t)((uint32_t)warp_incl_sum(sc, lane) + (uint32_t)prev_s);
+    int32_t cand = ts > prev_m ? ts : prev_m;
+    int32_t scanned = warp_incl_max(cand);
+    uint32_t dropped = __ballot_sync(0xffffffffu, (int32_t)((uint32_t)scanned - (uint32_t)ts) > X);
+    uint32_t first = dropped ? __ffs(dropped) - 1 : 32u;
+    int32_t mx = __shfl_sync(0xffffffffu, scanned, (first + 31) & 31);
+    if (first == 0) mx = prev_m;
+    int32_t pos;
+    if (mx == prev_m) {
+      pos = prev_pos;
+    } else {
+      uint32_t win = __ballot_sync(0xffffffffu, ts == mx && lane < first);
+      pos = (int32_t)(__ffs(win) - 1 + tile) + (LEFT ? 1 : 0);
+    }
+    if (dropped) {
+      *cells += min(tile + first + 1, nmax);
+      *out_max = mx;
+      *out_pos = pos;
+      return;
+    }
+    if (tile + 32 >= nmax) {  // the tile reached the edge
+      *cells += nmax;
+      *out_max = mx;
+      *out_pos = pos;
+      return;
+    }
+    prev_s = __shfl_sync(0xffffffffu, ts, 31);
+    prev_m = mx;
+    prev_pos = pos;
+  }
+}
+
+constexpr int kExactThreads = 128;
+
+__global__ void __launch_bounds__(kExactThreads) exact_kernel(ExactArgs a) {
+  __shared__ int32_t sub[64];
+  if (threadIdx.x < 64) sub[threadIdx.x] = a.sub[threadIdx.x];
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t ncand = min(a.tot->cand, a.cand_cap);
+  unsigned long long cells_acc = 0;
+  const uint32_t warps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t i = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; i < ncand; i += warps) {
+    Cand cd = a.cand[i];
+    bool is_long = cd.call & kLongFlag;
+    CallDev call = a.calls[cd.call & ~kLongFlag];
+    const uint8_t *qry = a.qbuf + call.qoff;
+    uint32_t q0 = cd.q0 - call.qoff, r0 = cd.r0;
+    unsigned long long cells = 0;
+    int32_t rmax, rpos, lmax, lpos;
+    exact_dir<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos, &cells);
+    exact_dir<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
+    if (is_long) cells_acc += cells;
+    int32_t total = (int32_t)((uint32_t)rmax + (uint32_t)lmax);
+    int32_t extent = (int32_t)((uint32_t)rpos + (uint32_t)lpos);
+    int32_t T = a.hspthresh;
+    int32_t T3 = (int32_t)((uint32_t)T * 3u);
+    double entropy = 1.0;
+    if (total >= T && total <= T3 && a.noentropy == 0) {
+      uint32_t rs = r0 - (uint32_t)lpos, qs = q0 - (uint32_t)lpos;
+      int32_t positions = (int32_t)((uint32_t)extent + 1u);
+      unsigned long long packed = 0;  // four 16-bit match counters, packed as the reference packs them
+      for (int32_t j = (int32_t)lane; j < positions; j += 32) {
+        uint32_t x = a.ref[rs + (uint32_t)j], y = qry[qs + (uint32_t)j];
+        if (x == y && x < 4) packed += 1ull << (16 * x);
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) packed += __shfl_xor_sync(0xffffffffu, packed, d);
+      int32_t c[4] = {(int32_t)(packed & 0xFFFF), (int32_t)((packed >> 16) & 0xFFFF),
+                      (int32_t)((packed >> 32) & 0xFFFF), (int32_t)((packed >> 48) & 0xFFFF)};
+      if (c[0] + c[1] + c[2] + c[3] >= 20) {
+        double denom = (double)((int32_t)((uint32_t)extent + 1u));
+        double ent = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          double pr = __ddiv_rn((double)c[j], denom);
+          double lg = c[j] != 0 ? hz_ln(pr) : 0.0;
+          ent = __dadd_rn(ent, __dmul_rn(pr, lg));
+        }
+        entropy = __ddiv_rn(-ent, 1.3862943649291992);  // (double)logf(4.0f), src/gpu/mod.rs:2349-2352
+      }
+    }
+    if (lane == 0 && sat_i32(__dmul_rn((double)__int2float_rn(total), entropy)) >= T) {
+      SegmentPair h;
+      h.ref_start = r0 - (uint32_t)lpos;
+      h.query_start = q0 - (uint32_t)lpos;
+      h.len = (uint32_t)extent;
+      h.score = entropy > 0.0 ? sat_i32(__dmul_rn((double)total, entropy)) : 0;
+      uint32_t at = atomicAdd(&a.tot->raw, 1u);
+      if (at < a.raw_cap) {
+        a.raw[at] = h;
+        a.raw_scope[at] = cd.scope;
+      }
+    }
+  }
+  if (lane == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
+}
+
+}  // namespace hz

@@ -16,7 +16,7 @@ from .hsp import PASS_RECORD, SEGMENT_PAIR
 from .scoring import build_sub_mat
 from .sequence import as_bytes
 
-BATCH_RECORD = np.dtype([("query", "<u4"), ("interval", "<u4"), ("strand", "<u4"), ("_pad", "<u4"),
+BATCH_RECORD = np.dtype([("query", "<u4"), ("interval", "<u4"), ("strand", "<u4"),
                          ("ref_start", "<u4"), ("query_start", "<u4"), ("len", "<u4"), ("score", "<i4")])
 
 
@@ -161,6 +161,24 @@ class Engine:
         N.check(N.lib().hz_run_pass(self._h, C.byref(out), C.byref(n), C.byref(st)))
         return _take(out, n.value, PASS_RECORD), st.as_dict()
 
+    # --- batched form ---------------------------------------------------------
+    def stage_queries(self, queries):
+        """Keep many ASCII query blocks resident (both strands encoded on the device)."""
+        arrs = [np.ascontiguousarray(as_bytes(q)) for q in queries]
+        qs = (N.QueryC * max(len(arrs), 1))()
+        for i, a in enumerate(arrs):
+            qs[i].ascii = a.ctypes.data if a.size else None
+            qs[i].len = a.size
+        N.check(N.lib().hz_stage_queries(self._h, qs, len(arrs)))
+        self._staged = arrs  # keep alive until the copies are done (they are synchronous)
+
+    def run_batched(self):
+        """Every call of every staged query through shared waves; records per
+        query in the same order run_pass gives for that query alone."""
+        out, n, st = C.c_void_p(), C.c_uint64(), N.StatsC()
+        N.check(N.lib().hz_run_batched(self._h, C.byref(out), C.byref(n), C.byref(st)))
+        return _take(out, n.value, BATCH_RECORD), st.as_dict()
+
     # --- profiling ----------------------------------------------------------
     def set_profiling(self, on: bool = True):
         N.check(N.lib().hz_engine_set_profiling(self._h, int(bool(on))))
@@ -182,6 +200,12 @@ class Engine:
         """Run on a caller-owned cudaStream_t (an int handle, e.g.
         torch.cuda.current_stream().cuda_stream); 0 restores the own stream."""
         N.check(N.lib().hz_engine_set_stream(self._h, C.c_void_p(stream_handle or None)))
+
+    def set_tuning(self, **knobs):
+        """Launch-shape knobs: gate_tile, gate_cap, gate_blocks_per_sm,
+        wave_positions.  Results never depend on them."""
+        for k, v in knobs.items():
+            N.check(N.lib().hz_engine_set_tuning(self._h, k.encode(), int(v)))
 
     @property
     def launches(self) -> int:

@@ -129,6 +129,33 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
  * call.  Records are grouped per interval, plus before minus, in call order. */
 int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats);
 
+/* One query block for the batched form (ASCII, records joined by '&'). */
+typedef struct hz_query {
+  const uint8_t *ascii;
+  uint64_t len;
+} hz_query;
+
+/* One record of a batched run: query index, interval, strand, HSP. */
+typedef struct hz_batch_record {
+  uint32_t query;
+  uint32_t interval;
+  uint32_t strand;
+  hz_segment_pair h;
+} hz_batch_record;
+
+/* Replaces the resident query store with `nq` query blocks (the reference
+ * swaps one query bin at a time, src/gpu/mod.rs:1142-1148; this keeps many
+ * resident).  Both strands are encoded on the device. */
+int hz_stage_queries(hz_engine *e, const hz_query *queries, uint32_t nq);
+
+/* Batched form of seed_and_filter_all (src/run.rs:266-495) over every staged
+ * query: all calls of many queries go through shared waves (one lookup, one
+ * persistent gate launch over a device work queue, one read-back per wave)
+ * instead of one launch chain per call.  Records are grouped by query, then
+ * exactly as hz_run_pass orders them; each query's records equal what
+ * hz_run_pass returns for that query alone. */
+int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *stats);
+
 /* dedup_and_order (src/hsp.rs:94-126) on host records, in place; returns
  * the kept count in *n_out. */
 int hz_dedup_and_order(hz_segment_pair *h, uint64_t n, uint64_t *n_out);
@@ -140,6 +167,13 @@ int hz_engine_set_profiling(hz_engine *e, int on);
 int hz_engine_profile_entry(hz_engine *e, uint32_t i, char *name, uint32_t name_cap, double *ms,
                             uint64_t *launches);
 int hz_engine_profile_reset(hz_engine *e);
+
+/* Launch-shape knobs (no reference counterpart; results never depend on
+ * them): "gate_tile" (hits per gate block tile: 1024, 2048, 4096),
+ * "gate_cap" (cells per direction before a hit goes to the warp kernel,
+ * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
+ * "wave_positions" (seed positions per batched wave). */
+int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
 
 /* Kernel launches issued by this engine since creation. */
 uint64_t hz_engine_launches(hz_engine *e);
