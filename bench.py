@@ -1,25 +1,33 @@
 #!/usr/bin/env python
 """Seed-and-filter benchmark on one node.
 
-Workload (the reference's "plain per-chunk at scale" configuration): a
-100 Mbp synthetic target split into 10 bins of 10 Mbp against a 100 Mbp
+Default workload (the reference's "plain per-chunk at scale" configuration):
+a 100 Mbp synthetic target split into 10 bins of 10 Mbp against a 100 Mbp
 synthetic query (41% GC, 10% soft-masked, 20,000 planted segments of
 200-5000 bp at 10-30% substitutions plus 1% small indels), 12of19 seed with
 one transition, HOXD70, X-drop 910, HSP threshold 3000, both strands.
-A step is one full pass: every bin x every interval x strand x WGA chunk.
+--config 3: a resident 200 Mbp target against 512 query chunks with
+log-uniform lengths in 10 kbp-2 Mbp carrying planted homology at 5-35%.
+
+A step is one full pass of every bin x every query x interval x strand x
+WGA chunk.  Two forms are timed: the plain per-chunk form (one launch chain
+and one read-back per seed_and_filter call, as the reference runs) and the
+batched form (all calls of a bin in shared waves: one lookup, one persistent
+gate launch over a device work queue, one read-back per wave).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--form plain|batched] [--scale S]
+                  [--config 2|3] [--form both|batched|plain] [--scale S]
 
-One JSON line on rank 0.  `value` is seed hits/s over all ranks with the
-targets and query resident in HBM; `e2e` is the same metric through the C
-ABI from pinned host buffers (uploads, on-device index builds and result
-read-back inside the timed region).  Multi-GPU runs are independent replicas
-(weak scaling; the path has no exchange step).
+One JSON line on rank 0.  `value` is seed hits/s over all ranks for the
+batched form with targets and queries resident in HBM; `e2e` is the same
+metric through the C ABI from pinned host buffers (uploads, on-device seed
+table builds, query encoding and result read-back inside the timed region).
+Multi-GPU runs are independent replicas (weak scaling; no exchange step).
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -29,8 +37,6 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-
-import numpy as np  # noqa: E402
 
 METRIC = "seed hits/s"
 UNIT = "hits/s"
@@ -45,19 +51,26 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def workload(scale: float):
+def workload(config: int, scale: float):
+    """(target bins, query blocks) as ASCII arrays."""
     from hspz_b200 import synth
+    if config == 3:
+        target, chunks = synth.config3(seed=3, scale=scale)
+        return [target], chunks
     bins, query = synth.config2(seed=2, scale=scale)
-    return bins, query
+    return bins, [query]
 
 
-def config_block(args, n_gpus):
-    return {"workload": "config2: 100 Mbp target as 10 bins x 10 Mbp vs 100 Mbp query, both strands"
-            if args.scale == 1.0 else f"config2 scaled x{args.scale}",
-            "target_bp": int(100_000_000 * args.scale), "query_bp": int(100_000_000 * args.scale),
-            "bins": 10, "seed": "12of19", "transitions": True, "xdrop": 910, "hspthresh": 3000,
-            "max_hits": 16711680, "wga_chunk": 250000, "interval": 10000000, "form": args.form,
-            "parallelism": f"replicas x{n_gpus}", "l2": "inputs larger than L2 (126 MB)"}
+def config_block(args, n_gpus, bins, queries):
+    name = ("config2: 100 Mbp target as 10 bins x 10 Mbp vs 100 Mbp query" if args.config == 2 else
+            "config3: 200 Mbp resident target vs 512 query chunks (log-uniform 10 kbp-2 Mbp)")
+    if args.scale != 1.0:
+        name += f", scaled x{args.scale}"
+    return {"workload": name + ", both strands", "target_bp": int(sum(b.size for b in bins)),
+            "query_bp": int(sum(q.size for q in queries)), "bins": len(bins), "queries": len(queries),
+            "seed": "12of19", "transitions": True, "xdrop": 910, "hspthresh": 3000, "max_hits": 16711680,
+            "wga_chunk": 250000, "interval": 10000000, "parallelism": f"replicas x{n_gpus}",
+            "l2": "inputs larger than L2 (126 MB)"}
 
 
 # ---------------------------------------------------------------------------
@@ -71,7 +84,7 @@ class Clocks:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}.csv")
+        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}_{device}.csv")
 
     def __enter__(self):
         try:
@@ -117,15 +130,17 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-def cpu_sample(bins, query, threads: int, budget_batches: int):
-    """The oracle (C restatement of the reference's path) on bin 0 x the first
-    `budget_batches` calls of the pass; returns (hits/s, stats, seconds)."""
+def cpu_sample(bins, queries, threads: int, budget_batches: int):
+    """The oracle (C restatement of the reference's path) on bin 0 x the
+    first `budget_batches` calls of query 0's pass, all host threads;
+    returns (hits/s, stats, seconds)."""
     import oracle
     from hspz_b200 import build_sub_mat
     from hspz_b200 import sequence as S
+    q = queries[0] if len(queries) == 1 else max(queries, key=lambda a: a.size)
     ref = oracle.encode(bins[0].tobytes())
-    qf = oracle.encode(query.tobytes())
-    qr = oracle.encode(S.reverse_complement_bytes(query).tobytes())
+    qf = oracle.encode(q.tobytes())
+    qr = oracle.encode(S.reverse_complement_bytes(q).tobytes())
     sh = oracle.shape("12of19")
     idx, pos = oracle.seed_table(ref, sh)
     p = oracle.params(build_sub_mat("", 910), threads=threads)
@@ -135,28 +150,33 @@ def cpu_sample(bins, query, threads: int, budget_batches: int):
     return st["hits"] / dt, st, dt
 
 
+def cpu_sample_text(args, st, dt):
+    return (f"bin 0 x the first {args.cpu_batches} seed_and_filter calls of the "
+            f"{'query' if args.config == 2 else 'longest query chunk'} ({st['hits']} hits, {dt:.1f} s)")
+
+
 def run_reference(args, rank):
-    """The reference arm: its CPU path (the oracle restatement; the Rust
-    reference cannot be built here and has no CPU extension path) on the host
-    cores, a bounded sample per step."""
+    """The reference arm: its CPU path -- the oracle restatement, since the
+    Rust reference cannot be built here and has no CPU extension path -- on
+    the host cores, a bounded sample per step."""
     if rank != 0:
         return
-    bins, query = workload(args.scale)
+    bins, queries = workload(args.config, args.scale)
     threads = os.cpu_count() or 1
     vals = []
-    st = None
+    st = dt = None
     for i in range(args.warmup + args.steps):
-        v, st, dt = cpu_sample(bins, query, threads, args.cpu_batches)
+        v, st, dt = cpu_sample(bins, queries, threads, args.cpu_batches)
         if i >= args.warmup:
             vals.append((v, dt))
     v = statistics.median([x[0] for x in vals])
     ms = statistics.median([x[1] for x in vals]) * 1000
-    sample = f"bin 0 x first {args.cpu_batches} of 80 calls of the pass ({st['hits']} hits)"
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": config_block(args, args.gpus),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "config": config_block(args, args.gpus, bins, queries),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": cpu_sample_text(args, st, dt)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -165,16 +185,17 @@ def run_reference(args, rank):
 def run_ours(args, rank, world, local_rank):
     import torch
     from hspz_b200 import Engine, EngineConfig
+    from hspz_b200 import _native as N
     from hspz_b200.build import build
 
-    if rank == 0 or world == 1:
+    if rank == 0:
         build()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream(dev)
-    bins, query = workload(args.scale)
+    bins, queries = workload(args.config, args.scale)
     cfg = EngineConfig()
 
     def barrier():
@@ -189,95 +210,136 @@ def run_ours(args, rank, world, local_rank):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident: one engine per bin, tables and query resident ----
+    # ---- device-resident: one engine per bin, target and queries resident ----
     engines = []
     for b in bins:
         e = Engine(cfg, device=local_rank)
         e.set_stream(stream.cuda_stream)
+        if args.tuning:
+            e.set_tuning(**json.loads(args.tuning))
         e.load_target(b)
-        e.swap_query_ascii(query)
+        e.stage_queries(queries)
         engines.append(e)
 
-    def step():
-        tot = {"hits": 0, "cells": 0, "raw_hsps": 0, "hsps": 0, "seeds": 0}
-        nrec = 0
+    def step(form):
+        tot = {"hits": 0, "cells": 0, "raw_hsps": 0, "hsps": 0, "seeds": 0, "calls": 0}
+        recs = []
         for e in engines:
-            recs, st = e.run_pass()
-            nrec += recs.size
-            for k in tot:
-                tot[k] += st[k]
-        return tot, nrec
+            if form == "batched":
+                r, st = e.run_batched()
+                recs.append(r)
+                for k in tot:
+                    tot[k] += st[k]
+            else:
+                for qi in range(len(queries)):
+                    e.select_query(qi)
+                    r, st = e.run_pass()
+                    recs.append(r)
+                    for k in tot:
+                        tot[k] += st[k]
+        return tot, recs
 
-    for _ in range(args.warmup):
-        step()
-    for e in engines:
-        e.set_profiling(True)
-        e.profile_reset()
-    l0 = sum(e.launches for e in engines)
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local_rank) as clk:
-        ev0.record(stream)
-        totals = []
-        for _ in range(args.steps):
-            totals.append(step())
-        ev1.record(stream)
+    def timed(form):
+        for _ in range(args.warmup):
+            step(form)
+        for e in engines:
+            e.set_profiling(True)
+            e.profile_reset()
+        l0 = sum(e.launches for e in engines)
         barrier()
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms)
-    launches = sum(e.launches for e in engines) - l0
-    prof = {}
-    for e in engines:
-        for k, (t, n) in e.profile().items():
-            a = prof.setdefault(k, [0.0, 0])
-            a[0] += t
-            a[1] += n
-        e.set_profiling(False)
-    tot, nrec = totals[-1]
-    hits_step = tot["hits"]
-    cells_step = tot["cells"]
-    value = hits_step * args.steps * world / (ms / 1000)
-    bp_s = cells_step * args.steps * world / (ms / 1000)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local_rank) as clk:
+            ev0.record(stream)
+            res = [step(form) for _ in range(args.steps)]
+            ev1.record(stream)
+            barrier()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        prof = {}
+        for e in engines:
+            for k, (t, n) in e.profile().items():
+                a = prof.setdefault(k, [0.0, 0])
+                a[0] += t
+                a[1] += n
+            e.set_profiling(False)
+        launches = sum(e.launches for e in engines) - l0
+        tot, recs = res[-1]
+        return {"ms": ms, "tot": tot, "recs": recs, "prof": prof, "launches": launches, "clocks": clk.summary()}
 
-    # roofline of the dominant kernel (the X-drop extension): algorithmic
-    # bytes = 2 B per scored cell (1 B reference + 1 B query code)
+    forms = ["batched", "plain"] if args.form == "both" else [args.form]
+    runs = {f: timed(f) for f in forms}
+    if len(runs) == 2:
+        a, b = runs["batched"]["recs"], runs["plain"]["recs"]
+        # per bin the batched records of query q equal the plain records of q
+        import numpy as np
+        same = True
+        for bi in range(len(bins)):
+            br = a[bi]
+            pr = b[bi * len(queries):(bi + 1) * len(queries)]
+            for qi, p in enumerate(pr):
+                sel = br[br["query"] == qi]
+                for f in ("interval", "strand", "ref_start", "query_start", "len", "score"):
+                    if not np.array_equal(sel[f], p[f]):
+                        same = False
+        if not same:
+            raise SystemExit("batched and plain forms disagree")
+
     peak, peak_kind = peaks()
-    ext_ms, ext_n = prof.get("extend", (0.0, 0))
-    ext_bytes = 2.0 * cells_step * args.steps
-    ext_avg_ms = ext_ms / max(ext_n, 1)
-    achieved = (ext_bytes / max(ext_n, 1)) / (ext_avg_ms / 1000) / 1e9 if ext_ms > 0 else None
+
+    def summarize(r):
+        ms, tot, prof = r["ms"], r["tot"], r["prof"]
+        per_s = args.steps * world / (ms / 1000)
+        gate_ms, gate_n = prof.get("gate", (0.0, 0))
+        # dominant kernel: the fused expansion + X-drop gate.  Algorithmic
+        # bytes: 2 B per scored cell (reference + query code) + 4 B per hit
+        # (its pos_table entry).
+        gate_bytes = (2.0 * tot["cells"] + 4.0 * tot["hits"]) * args.steps
+        gate_gbs = gate_bytes / (gate_ms / 1000) / 1e9 if gate_ms else None
+        lk_ms = prof.get("lookup_count", (0.0, 0))[0]
+        # seed lookup: 1 B per query position + 8 B per seed (two index words)
+        positions = tot["seeds"] / 13.0
+        lk_bytes = (positions * 1.0 + tot["seeds"] * 8.0) * args.steps
+        lk_gbs = lk_bytes / (lk_ms / 1000) / 1e9 if lk_ms else None
+        return {"hits_per_s": tot["hits"] * per_s, "extended_bp_per_s": tot["cells"] * per_s,
+                "ms_per_step": ms / args.steps, "hits_per_step": tot["hits"], "cells_per_step": tot["cells"],
+                "hsps_per_step": tot["hsps"], "raw_hsps_per_step": tot["raw_hsps"], "calls_per_step": tot["calls"],
+                "gpu_launches": r["launches"],
+                "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in prof.items()},
+                "kernel_launches_per_step": {k: v[1] // args.steps for k, v in prof.items()},
+                "gate": {"achieved": gate_gbs, "avg_launch_ms": gate_ms / max(gate_n, 1),
+                         "bytes_per_launch": gate_bytes / max(gate_n, 1)},
+                "lookup": {"achieved": lk_gbs, "frac": lk_gbs / peak if lk_gbs else None},
+                "clocks": r["clocks"]}
+
+    summ = {f: summarize(r) for f, r in runs.items()}
+    head = summ["batched"] if "batched" in summ else summ["plain"]
+    head_form = "batched" if "batched" in summ else "plain"
+
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "extend_traffic.json")
-    if os.path.exists(tfile) and ext_n:
+    tfile = os.path.join(ROOT, "profiles", "gate_traffic.json")
+    if os.path.exists(tfile):
         tr = json.load(open(tfile))
-        traffic = tr["dram_bytes_per_cell"] * cells_step * args.steps / ext_n
-    lookup_names = ("seed_count", "pair", "scan", "seed_compact", "expand")
-    lk_ms = sum(prof.get(k, (0.0, 0))[0] for k in lookup_names)
-    seeds_step = tot["seeds"]
-    # B_lookup = 1 B/query base per strand + 8 B per seed (two index words) + 4 B per hit (pos_table)
-    # + 8 B per hit (anchors written by expand)
-    qlen = query.size
-    lk_bytes = (2 * qlen * len(bins) + 8 * seeds_step + 12 * hits_step) * args.steps
-    lookup_gbs = lk_bytes / (lk_ms / 1000) / 1e9 if lk_ms > 0 else None
+        traffic = tr.get("dram_bytes_per_hit", 0) * head["hits_per_step"] * args.steps / max(
+            runs[head_form]["prof"].get("gate", (0, 1))[1], 1)
 
     # ---- end to end through the C ABI from pinned host buffers ------------
     e2e = None
     if not args.no_e2e:
-        pin_q = torch.from_numpy(query).pin_memory()
-        pin_bins = [torch.from_numpy(b).pin_memory() for b in bins]
+        pin_q = [torch.from_numpy(q).pin_memory() for q in queries]
+        pin_b = [torch.from_numpy(b).pin_memory() for b in bins]
         e2 = Engine(cfg, device=local_rank)
         e2.set_stream(stream.cuda_stream)
-        from hspz_b200 import _native as N
-        import ctypes as C
         L = N.lib()
+        qarr = (N.QueryC * len(pin_q))()
+        for i, t in enumerate(pin_q):
+            qarr[i].ascii = t.data_ptr() if t.numel() else None
+            qarr[i].len = t.numel()
 
         def e2e_step():
-            N.check(L.hz_swap_query_ascii(e2._h, C.c_void_p(pin_q.data_ptr()), pin_q.numel()))
-            hits = 0
-            d2h = 0
-            for pb in pin_bins:
+            hits = d2h = 0
+            for pb in pin_b:  # per reference bin: Engine::new + swap_query (src/run.rs:816-887)
                 N.check(L.hz_engine_load_target(e2._h, C.c_void_p(pb.data_ptr()), pb.numel()))
-                recs, st = e2.run_pass()
+                N.check(L.hz_stage_queries(e2._h, qarr, len(pin_q)))
+                recs, st = e2.run_batched()
                 hits += st["hits"]
                 d2h += recs.nbytes
             return hits, d2h
@@ -285,45 +347,43 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(max(1, args.warmup)):
             e2e_step()
         barrier()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         res = [e2e_step() for _ in range(args.steps)]
         t1.record(stream)
         barrier()
         ems = max_over_ranks(t0.elapsed_time(t1))
-        hits_e = res[-1][0]
-        e2e = {"value": hits_e * args.steps * world / (ems / 1000), "unit": UNIT,
-               "h2d_bytes_per_step": int(pin_q.numel() + sum(p.numel() for p in pin_bins)),
-               "d2h_bytes_per_step": int(res[-1][1]), "ms_per_step": ems / args.steps}
+        e2e = {"value": res[-1][0] * args.steps * world / (ems / 1000), "unit": UNIT,
+               "h2d_bytes_per_step": int(sum(p.numel() for p in pin_b) + len(pin_b) * sum(p.numel() for p in pin_q)),
+               "d2h_bytes_per_step": int(res[-1][1]), "ms_per_step": ems / args.steps, "form": "batched"}
         e2.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, st, dt = cpu_sample(bins, query, threads, args.cpu_batches)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"bin 0 x first {args.cpu_batches} of 80 calls of the pass ({st['hits']} hits, {dt:.1f} s)"}
+        v, st, dt = cpu_sample(bins, queries, threads, args.cpu_batches)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": cpu_sample_text(args, st, dt)}
 
     for e in engines:
         e.close()
     if rank != 0:
         return
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+    g = head["gate"]
+    line = {"metric": METRIC, "value": head["hits_per_s"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": config_block(args, world),
-            "extended_bp_per_s": bp_s, "hits_per_step": hits_step, "cells_per_step": cells_step,
-            "hsps_per_step": tot["hsps"], "raw_hsps_per_step": tot["raw_hsps"],
-            "roofline": {"bound": "hbm", "kernel": "extend", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None, "traffic": traffic,
+            "config": dict(config_block(args, world, bins, queries), form=head_form),
+            "extended_bp_per_s": head["extended_bp_per_s"],
+            "roofline": {"bound": "hbm", "kernel": "gate (fused hit expansion + X-drop score gate)",
+                         "achieved": g["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": g["achieved"] / peak if g["achieved"] else None, "traffic": traffic,
                          "peak_kind": peak_kind,
-                         "note": "X-drop extension is issue-bound; algorithmic bytes = 2 B per scored cell"},
-            "lookup_roofline": {"kernels": list(lookup_names), "achieved": lookup_gbs, "peak": peak, "unit": "GB/s",
-                                "frac": lookup_gbs / peak if lookup_gbs else None},
-            "kernel_ms": {k: round(v[0], 3) for k, v in prof.items()},
-            "kernel_launches": {k: v[1] for k, v in prof.items()},
-            "gpu_launches": launches, "clocks": clk.summary(), "e2e": e2e, "cpu_baseline": cpu}
+                         "note": "issue-bound integer kernel; algorithmic bytes = 2 B per scored cell + 4 B per hit"},
+            "lookup_roofline": dict(head["lookup"], kernel="lookup_count", peak=peak, unit="GB/s"),
+            "forms": summ,
+            "batched_over_plain": (summ["batched"]["hits_per_s"] / summ["plain"]["hits_per_s"]
+                                   if len(summ) == 2 else None),
+            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"], "e2e": e2e, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
 
 
@@ -333,9 +393,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain"])
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3])
+    ap.add_argument("--form", default="both", choices=["both", "batched", "plain"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-batches", type=int, default=80)
+    ap.add_argument("--tuning", default="", help='JSON of engine launch knobs, e.g. {"gate_tile": 4096}')
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -78,6 +78,7 @@ SIGNATURES = {
     "hz_run_pass": (C.c_int, [P, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_dedup_and_order": (C.c_int, [P, U64, PU64]),
     "hz_stage_queries": (C.c_int, [P, C.POINTER(QueryC), U32]),
+    "hz_select_query": (C.c_int, [P, U32]),
     "hz_run_batched": (C.c_int, [P, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_engine_set_profiling": (C.c_int, [P, C.c_int]),
     "hz_engine_profile_entry": (C.c_int, [P, U32, C.c_char_p, U32, C.POINTER(C.c_double), PU64]),

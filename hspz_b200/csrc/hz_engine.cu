@@ -255,6 +255,7 @@ struct hz_engine {
   SeqBuf qstore;
   DBuf<uint8_t> qascii;
   std::vector<StagedQuery> queries;
+  uint32_t cur_query = 0;  // the query the per-call entry points work on
   bool has_query = false;
   Slot slot[2];
   // wave buffers
@@ -271,7 +272,7 @@ struct hz_engine {
   HBuf<uint32_t> h_raw_scope, h_scope_call;
   uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
   // tuning
-  int gate_tile = 2048;
+  int gate_tile = 1024;
   uint32_t gate_cap = 256;
   int gate_blocks_per_sm = 0;
   uint64_t wave_positions = 1ull << 27;  // seed positions per batched wave
@@ -444,6 +445,8 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     ga.cand = e->cand.p;
     ga.cand_cap = e->cand_cap;
     switch (e->gate_tile) {
+      case 512: TRY(launch_gate<512>(e, ga)); break;
+      case 768: TRY(launch_gate<768>(e, ga)); break;
       case 1024: TRY(launch_gate<1024>(e, ga)); break;
       case 4096: TRY(launch_gate<4096>(e, ga)); break;
       default: TRY(launch_gate<2048>(e, ga)); break;
@@ -578,6 +581,7 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
   }
   TRY(e->sync());
   e->queries = qs;
+  e->cur_query = 0;
   e->has_query = nq > 0;
   e->slot[0].kind = e->slot[1].kind = 0;
   return HZ_OK;
@@ -585,7 +589,7 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
 
 int check_range(hz_engine *e, uint32_t start, uint32_t end) {
   if (end < start) return fail(HZ_E_INVALID, "seed range [%u, %u) is reversed", start, end);
-  uint32_t qlen = e->queries.empty() ? 0 : e->queries[0].len;
+  uint32_t qlen = e->queries.empty() ? 0 : e->queries[e->cur_query].len;
   if (end > start && (uint64_t)end + e->shape.size - 1 > qlen)
     return fail(HZ_E_INVALID, "seed range [%u, %u) exceeds query length %u", start, end, qlen);
   return HZ_OK;
@@ -902,6 +906,7 @@ int hz_swap_query(hz_engine *e, const uint8_t *query, const uint8_t *query_rc, u
   }
   TRY(e->sync());
   e->queries.assign(1, q);
+  e->cur_query = 0;
   e->has_query = true;
   e->slot[0].kind = e->slot[1].kind = 0;
   return HZ_OK;
@@ -917,7 +922,7 @@ int hz_upload_seeds(hz_engine *e, uint32_t slot, const uint64_t *seeds, uint64_t
   if (!e || slot > 1 || (n && !seeds)) return fail(HZ_E_INVALID, "bad argument");
   if (!e->has_query) return fail(HZ_E_STATE, "Engine has no query: swap_query() must be called before upload_seeds()");
   if (n >= 0x7FFFFFFFull) return fail(HZ_E_INVALID, "too many seeds in one call");
-  uint32_t qlen = e->queries[0].len;
+  uint32_t qlen = e->queries[e->cur_query].len;
   uint32_t max_pos = qlen >= e->shape.size ? qlen - e->shape.size : 0;
   for (uint64_t i = 0; i < n; i++) {
     uint64_t k = seeds[i] >> 32;
@@ -953,7 +958,7 @@ int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint
   uint64_t nv = 0;
   if (end > start) {
     // the lookup kernel counts valid windows as it goes: run it alone
-    const StagedQuery &q = e->queries[0];
+    const StagedQuery &q = e->queries[e->cur_query];
     TRY(e->h_calls.ensure(1));
     e->h_calls.p[0] = CallDev{s.rev ? q.off_r : q.off_f, q.len, start, 0};
     TRY(e->calls.ensure(1, e->st));
@@ -1003,10 +1008,10 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
   memset(&local, 0, sizeof local);
   std::vector<WaveRecord> recs;
   if (s.kind == 2) {
-    HostCall hc{0, 0, (uint32_t)(rev ? 1 : 0), s.start, s.end};
+    HostCall hc{e->cur_query, 0, (uint32_t)(rev ? 1 : 0), s.start, s.end};
     TRY(run_wave(e, &hc, s.end > s.start ? 1 : 0, nullptr, s.transitions, &recs, &local));
   } else if (s.n) {
-    HostCall hc{0, 0, (uint32_t)(rev ? 1 : 0), 0, (uint32_t)s.n};
+    HostCall hc{e->cur_query, 0, (uint32_t)(rev ? 1 : 0), 0, (uint32_t)s.n};
     TRY(run_wave(e, &hc, 1, s.seeds.p, 0, &recs, &local));
   }
   local.seeds = s.n;
@@ -1027,7 +1032,7 @@ int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats
   hz_stats local;
   memset(&local, 0, sizeof local);
   std::vector<HostCall> calls;
-  query_calls(e, 0, &calls);
+  query_calls(e, e->cur_query, &calls);
   std::vector<WaveRecord> recs;
   for (size_t i = 0; i < calls.size(); i++) {
     size_t before = recs.size();
@@ -1058,6 +1063,14 @@ int hz_stage_queries(hz_engine *e, const hz_query *queries, uint32_t nq) {
   }
   TRY(set_device(e));
   return stage_ascii(e, ptrs.data(), lens.data(), nq);
+}
+
+int hz_select_query(hz_engine *e, uint32_t index) {
+  if (!e) return fail(HZ_E_INVALID, "null engine");
+  if (index >= e->queries.size()) return fail(HZ_E_INVALID, "query %u not staged (%zu staged)", index, e->queries.size());
+  e->cur_query = index;
+  e->slot[0].kind = e->slot[1].kind = 0;
+  return HZ_OK;
 }
 
 // The batched form: the calls of all staged queries, query-major, cut into
@@ -1141,7 +1154,8 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   if (!e || !key) return fail(HZ_E_INVALID, "null argument");
   std::string k(key);
   if (k == "gate_tile") {
-    if (value != 1024 && value != 2048 && value != 4096) return fail(HZ_E_INVALID, "gate_tile must be 1024, 2048 or 4096");
+    if (value != 512 && value != 768 && value != 1024 && value != 2048 && value != 4096)
+      return fail(HZ_E_INVALID, "gate_tile must be 512, 768, 1024, 2048 or 4096");
     e->gate_tile = (int)value;
   } else if (k == "gate_cap") {
     if (value < 8 || value > 65528 || value % 8) return fail(HZ_E_INVALID, "gate_cap must be a multiple of 8 in 8..65528");

@@ -1,0 +1,413 @@
+// Gate kernel of the wave pipeline (included by hz_wave.cuh).
+//
+// A persistent grid takes tiles of consecutive wave hits from a device work
+// queue.  Per tile it
+//   (1) recomputes the seeds of the positions covering the tile and records
+//       the (position, seed) slots that overlap it;
+//   (2) gives every hit its slot by a block max-scan of slot-start marks and
+//       stores, per hit, the reference and query anchors, the distances to
+//       the sequence edges and the call -- so that a lane picking up a hit
+//       later touches shared memory only;
+//   (3) runs the X-drop score gate thread-per-hit, first all right
+//       extensions and then all left extensions.  Before each pass the block
+//       gathers every hit's first eight cells of both sequences (and the
+//       next word), so a lane's first step needs no global load; each lane
+//       refills from the tile when its extension ends, so extensions of
+//       different lengths do not idle the warp, and it fetches the words of
+//       its next eight cells one step ahead.
+// Anchors are the END of the seed window on both sides (pos + seed_size,
+// src/gpu/kernels.rs:397-401).  A hit becomes a candidate when
+// (i32)(f32)(right max + left max) >= hspthresh -- the reference gate's bound
+// (src/gpu/kernels.rs:1048-1052), never below the final score since the
+// entropy factor is <= 1 -- or when an extension runs past `cap` cells
+// ("long"; the exact kernel redoes it warp-wide).
+#pragma once
+
+namespace hz {
+
+// Shared memory of one gate block.  The per-tile setup arrays and the
+// per-pass "first eight cells" arrays are never live at the same time.
+template <int TILE>
+struct GateSmem {
+  int32_t sub[64];
+  union {
+    struct {
+      uint32_t slot_bst[TILE];  // pos_table index of the slot's first in-tile hit
+      uint32_t slot_q[TILE];    // query anchor (absolute)
+      uint32_t slot_call[TILE];
+      uint32_t hit_slot[TILE];  // first hit of the hit's slot + 1 (mark, then max-scan)
+    } setup;
+    struct {
+      uint4 first[TILE];   // first eight cells: reference words a, b; query words a, b
+      uint2 carry[TILE];   // the next reference / query word of the stream
+    } pass;
+  } u;
+  uint32_t hit_r[TILE];     // reference anchor
+  uint32_t hit_q[TILE];     // query anchor (absolute)
+  uint32_t hit_n[TILE];     // cells to the right edge | cells to the left edge << 16 (each saturated)
+  uint32_t hit_call[TILE];
+  int32_t hit_rmax[TILE];   // right-extension maximum, or kSpilled
+  uint16_t hit_rcells[TILE];
+  uint32_t warp_tot[kScanThreads / 32];
+  unsigned long long h0;
+  uint32_t next, e0, e1;
+};
+constexpr int32_t kSpilled = -1;  // a right maximum is never negative
+
+struct GateArgs {
+  WaveIn w;
+  const unsigned long long *np_excl;
+  const uint32_t *np_pos;
+  const unsigned long long *scope_lo;
+  uint32_t scope_cap;  // entries of scope_lo (a wave with more scopes is rerun)
+  WaveTotals *tot;
+  int32_t sub[64];
+  int32_t xdrop;
+  int32_t hspthresh;
+  uint32_t cap;  // cells per direction before a hit goes to the exact kernel (multiple of 8, < 65536)
+  Cand *cand;
+  uint32_t cand_cap;
+};
+
+__device__ __forceinline__ const uint32_t *word_ptr(const uint8_t *p) {
+  return reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)3);
+}
+
+// Inclusive max-scan of the slot marks over the tile.
+template <int TILE>
+__device__ __forceinline__ void mark_scan(GateSmem<TILE> &sm, uint32_t nt) {
+  constexpr int PER = TILE / kScanThreads;
+  uint32_t *mark = sm.u.setup.hit_slot;
+  uint32_t base = threadIdx.x * PER;
+  uint32_t run = 0;
+#pragma unroll
+  for (int i = 0; i < PER; i++)
+    if (base + i < nt) run = max(run, mark[base + i]);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t incl = run;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl = max(incl, up);
+  }
+  if (lane == 31) sm.warp_tot[wid] = incl;
+  __syncthreads();
+  uint32_t carry = 0;
+  for (int i = 0; i < wid; i++) carry = max(carry, sm.warp_tot[i]);
+  uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane > 0) carry = max(carry, ex);
+#pragma unroll
+  for (int i = 0; i < PER; i++)
+    if (base + i < nt) {
+      carry = max(carry, mark[base + i]);
+      mark[base + i] = carry;
+    }
+}
+
+__device__ __forceinline__ uint32_t scope_of(const unsigned long long *scope_lo, uint32_t nscopes,
+                                             unsigned long long h) {
+  uint32_t lo = 0, hi = nscopes;  // last scope with scope_lo <= h
+  while (hi - lo > 1) {
+    uint32_t m = (lo + hi) >> 1;
+    if (scope_lo[m] <= h) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+// The eight bytes [p, p+8) (right) or [p-8, p) reversed (left) as two words,
+// cell 0 in the low byte, plus the word the next step continues from.
+template <bool LEFT>
+__device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint32_t *a, uint32_t *b,
+                                            uint32_t *carry) {
+  const uint32_t sh = (p & 3u) * 8u;
+  if (!LEFT) {
+    const uint32_t *w = word_ptr(seq + p);
+    uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+    *a = __funnelshift_r(w0, w1, sh);
+    *b = __funnelshift_r(w1, w2, sh);
+    *carry = w2;
+  } else {
+    const uint32_t *w = word_ptr(seq + p - 8);
+    uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+    *a = __byte_perm(__funnelshift_r(w1, w2, sh), 0, 0x0123);
+    *b = __byte_perm(__funnelshift_r(w0, w1, sh), 0, 0x0123);
+    *carry = w0;
+  }
+}
+
+// Scores one cell whose byte offset into the substitution table is byte SH
+// of T; keeps every running sum S and maximum M for the termination path
+// and the group's largest M - S in D.
+#define HZ_CELL(T, SH, I)                                                            \
+  {                                                                                  \
+    int32_t sc = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH)) & 0xFFu)); \
+    S = (int32_t)((uint32_t)S + (uint32_t)sc);                                       \
+    M = max(M, S);                                                                   \
+    Si[I] = S;                                                                       \
+    Mi[I] = M;                                                                       \
+    D = max(D, (int32_t)((uint32_t)M - (uint32_t)S));                                \
+  }
+
+template <int TILE, bool LEFT>
+__device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm, uint32_t nt,
+                                           unsigned long long &cells_acc) {
+  const uint8_t *ref = a.w.ref;
+  const uint8_t *qbuf = a.w.qbuf;
+  const char *subb = reinterpret_cast<const char *>(sm.sub);
+  const int32_t X = a.xdrop;
+  const uint32_t lane = threadIdx.x & 31;
+  bool have = false, exhausted = false, capped = false;
+  uint32_t t = 0, n = 0;
+  int32_t S = 0, M = 0;
+  uint32_t cells = 0;
+  // word stream state: the group about to be scored (ra, rb, qa, qb), the
+  // carried word and the two prefetched words of the following group
+  uint32_t ra = 0, rb = 0, qa = 0, qb = 0;
+  uint32_t rc = 0, r1 = 0, r2 = 0, qc = 0, q1 = 0, q2 = 0;
+  const uint32_t *wr = nullptr, *wq = nullptr;
+  uint32_t sr = 0, sq = 0;
+  while (true) {
+    if (!exhausted) {
+      unsigned need = __ballot_sync(0xffffffffu, !have);
+      if (need) {
+        int leader = __ffs(need) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(&sm.next, (uint32_t)__popc(need));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (base + __popc(need) >= nt) exhausted = true;
+        if (!have) {
+          uint32_t mine = base + __popc(need & lanemask_lt());
+          if (mine < nt && !(LEFT && sm.hit_rmax[mine] == kSpilled)) {
+            have = true;
+            t = mine;
+            const uint32_t r0 = sm.hit_r[t], q0 = sm.hit_q[t];
+            n = LEFT ? (sm.hit_n[t] >> 16) : (sm.hit_n[t] & 0xFFFFu);
+            capped = n > a.cap;
+            if (capped) n = a.cap;
+            S = 0;
+            M = 0;
+            cells = 0;
+            uint4 f = sm.u.pass.first[t];
+            uint2 cw = sm.u.pass.carry[t];
+            ra = f.x;
+            rb = f.y;
+            qa = f.z;
+            qb = f.w;
+            rc = cw.x;
+            qc = cw.y;
+            sr = (r0 & 3u) * 8u;
+            sq = (q0 & 3u) * 8u;
+            if (!LEFT) {
+              wr = word_ptr(ref + r0) + 2;  // the carried word
+              wq = word_ptr(qbuf + q0) + 2;
+              r1 = __ldg(wr + 1);
+              r2 = __ldg(wr + 2);
+              q1 = __ldg(wq + 1);
+              q2 = __ldg(wq + 2);
+            } else {
+              wr = word_ptr(ref + r0 - 8);  // the carried word
+              wq = word_ptr(qbuf + q0 - 8);
+              r1 = __ldg(wr - 1);
+              r2 = __ldg(wr - 2);
+              q1 = __ldg(wq - 1);
+              q2 = __ldg(wq - 2);
+            }
+          }
+        }
+      }
+    }
+    // (in the left pass a refill may hand out only hits that were spilled in
+    // the right pass, so an idle warp ends only once the tile is exhausted)
+    if (!__any_sync(0xffffffffu, have) && exhausted) break;
+    if (!have) continue;
+    // ---- eight cells ----
+    // codes are 0..7, so (r << 5) | (q << 2) is the byte offset of sub[r*8+q]
+    const uint32_t ta = (ra << 5) | (qa << 2), tb = (rb << 5) | (qb << 2);
+    // the next group from the carried and prefetched words; prefetch again
+    uint32_t nra, nrb, nqa, nqb;
+    if (!LEFT) {
+      nra = __funnelshift_r(rc, r1, sr);
+      nrb = __funnelshift_r(r1, r2, sr);
+      nqa = __funnelshift_r(qc, q1, sq);
+      nqb = __funnelshift_r(q1, q2, sq);
+      rc = r2;
+      qc = q2;
+      wr += 2;
+      wq += 2;
+    } else {
+      nra = __byte_perm(__funnelshift_r(r1, rc, sr), 0, 0x0123);
+      nrb = __byte_perm(__funnelshift_r(r2, r1, sr), 0, 0x0123);
+      nqa = __byte_perm(__funnelshift_r(q1, qc, sq), 0, 0x0123);
+      nqb = __byte_perm(__funnelshift_r(q2, q1, sq), 0, 0x0123);
+      rc = r2;
+      qc = q2;
+      wr -= 2;
+      wq -= 2;
+    }
+    const int32_t Ms = M;
+    int32_t Si[8], Mi[8];
+    int32_t D = 0;
+    HZ_CELL(ta, 0, 0)
+    HZ_CELL(ta, 8, 1)
+    HZ_CELL(ta, 16, 2)
+    HZ_CELL(ta, 24, 3)
+    HZ_CELL(tb, 0, 4)
+    HZ_CELL(tb, 8, 5)
+    HZ_CELL(tb, 16, 6)
+    HZ_CELL(tb, 24, 7)
+    if (D <= X && n > 8) {  // no drop and more cells left: advance the stream
+      n -= 8;
+      cells += 8;
+      ra = nra;
+      rb = nrb;
+      qa = nqa;
+      qb = nqb;
+      if (n > 8) {  // words of the group after next (never beyond the padding)
+        if (!LEFT) {
+          r1 = __ldg(wr + 1);
+          r2 = __ldg(wr + 2);
+          q1 = __ldg(wq + 1);
+          q2 = __ldg(wq + 2);
+        } else {
+          r1 = __ldg(wr - 1);
+          r2 = __ldg(wr - 2);
+          q1 = __ldg(wq - 1);
+          q2 = __ldg(wq - 2);
+        }
+      }
+      continue;
+    }
+    // The extension ends in this group: at the first valid cell with
+    // M - S > xdrop (keeping the maximum from before it), or after the v
+    // valid cells left before the edge or the cap.
+    const uint32_t v = min(n, 8u);
+    uint32_t dm = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
+    dm &= (1u << v) - 1u;
+    const uint32_t stop = dm ? (uint32_t)(__ffs(dm) - 1) : v;
+    int32_t res = Ms;
+#pragma unroll
+    for (int i = 1; i <= 8; i++)
+      if ((uint32_t)i == stop) res = Mi[i - 1];
+    cells += dm ? stop + 1 : v;
+    const bool spill = !dm && capped;
+    if (spill) {
+      uint32_t at = atomicAdd(&a.tot->cand, 1u);
+      if (at < a.cand_cap)
+        a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), sm.hit_r[t],
+                          sm.hit_q[t], sm.hit_call[t] | kLongFlag};
+      if (!LEFT) sm.hit_rmax[t] = kSpilled;  // the left pass skips it
+    } else if (!LEFT) {
+      sm.hit_rmax[t] = res;
+      sm.hit_rcells[t] = (uint16_t)cells;
+    } else {
+      cells_acc += cells + sm.hit_rcells[t];
+      int32_t total = (int32_t)((uint32_t)sm.hit_rmax[t] + (uint32_t)res);
+      if (sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
+        uint32_t at = atomicAdd(&a.tot->cand, 1u);
+        if (at < a.cand_cap)
+          a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), sm.hit_r[t],
+                            sm.hit_q[t], sm.hit_call[t]};
+      }
+    }
+    have = false;
+  }
+}
+
+// Fills the first eight cells and the carried word of every hit for one pass.
+template <int TILE, bool LEFT>
+__device__ __forceinline__ void prepare_pass(const GateArgs &a, GateSmem<TILE> &sm, uint32_t nt) {
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    if (LEFT && sm.hit_rmax[i] == kSpilled) continue;
+    uint32_t ra, rb, rc, qa, qb, qc;
+    first_group<LEFT>(a.w.ref, sm.hit_r[i], &ra, &rb, &rc);
+    first_group<LEFT>(a.w.qbuf, sm.hit_q[i], &qa, &qb, &qc);
+    sm.u.pass.first[i] = make_uint4(ra, rb, qa, qb);
+    sm.u.pass.carry[i] = make_uint2(rc, qc);
+  }
+}
+
+template <int TILE>
+__global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
+  static_assert(TILE % kScanThreads == 0, "tile must be a multiple of the block");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GateSmem<TILE> &sm = *reinterpret_cast<GateSmem<TILE> *>(smem_raw);
+  if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
+  unsigned long long cells_acc = 0;
+  const unsigned long long total = a.tot->hits;
+  const uint32_t nz = a.tot->nz;
+  const WaveIn &w = a.w;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) sm.h0 = atomicAdd(&a.tot->tiles, 1ull) * (unsigned long long)TILE;
+    __syncthreads();
+    const unsigned long long h0 = sm.h0;
+    if (h0 >= total) break;
+    const uint32_t nt = (uint32_t)min((unsigned long long)TILE, total - h0);
+    // positions covering [h0, h0 + nt)
+    if (threadIdx.x < 2) {
+      unsigned long long h = threadIdx.x == 0 ? h0 : h0 + nt - 1;
+      uint32_t k = last_le(a.np_excl, 0, nz, h);
+      if (threadIdx.x == 0) sm.e0 = k; else sm.e1 = k;
+    }
+    if (threadIdx.x == 0) sm.next = 0;
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) sm.u.setup.hit_slot[i] = 0;
+    __syncthreads();
+    // (1) slots overlapping the tile
+    const uint32_t e0 = sm.e0, e1 = sm.e1;
+    for (uint32_t k = e0 + threadIdx.x; k <= e1; k += blockDim.x) {
+      uint32_t p = a.np_pos[k];
+      uint32_t c = call_of(w.calls, w.ncalls, p);
+      CallDev cd = w.calls[c];
+      uint32_t qpos, kmer;
+      position_seed(w, cd, p, &qpos, &kmer);
+      unsigned long long lo = a.np_excl[k];
+      for (uint32_t v = 0; v < w.per_pos; v++) {
+        uint32_t beg;
+        uint32_t cnt = bucket(w, seed_variant(kmer, v), &beg);
+        unsigned long long hi = lo + cnt;
+        if (cnt && hi > h0 && lo < h0 + nt) {
+          unsigned long long first = lo > h0 ? lo : h0;
+          uint32_t s = (uint32_t)(first - h0);
+          sm.u.setup.slot_bst[s] = beg + (uint32_t)(first - lo);
+          sm.u.setup.slot_q[s] = cd.qoff + qpos + w.shape.size;
+          sm.u.setup.slot_call[s] = c;
+          sm.u.setup.hit_slot[s] = s + 1;
+        }
+        lo = hi;
+      }
+    }
+    __syncthreads();
+    // (2) per hit: slot, anchors, edge distances, call
+    mark_scan<TILE>(sm, nt);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+      uint32_t s = sm.u.setup.hit_slot[i] - 1;
+      uint32_t r0 = __ldg(w.pos_table + sm.u.setup.slot_bst[s] + (i - s)) + w.shape.size;
+      uint32_t q0 = sm.u.setup.slot_q[s];
+      uint32_t c = sm.u.setup.slot_call[s];
+      const CallDev &cd = w.calls[c];
+      uint32_t nr = min(w.rlen - r0, cd.qoff + cd.qlen - q0);
+      uint32_t nl = min(r0, q0 - cd.qoff);
+      sm.hit_r[i] = r0;
+      sm.hit_q[i] = q0;
+      sm.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
+      sm.hit_call[i] = c;
+    }
+    __syncthreads();
+    // (3) the score gate: right pass, then left pass
+    prepare_pass<TILE, false>(a, sm, nt);
+    __syncthreads();
+    gate_phase<TILE, false>(a, sm, nt, cells_acc);
+    __syncthreads();
+    if (threadIdx.x == 0) sm.next = 0;
+    prepare_pass<TILE, true>(a, sm, nt);
+    __syncthreads();
+    gate_phase<TILE, true>(a, sm, nt, cells_acc);
+  }
+  for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
+  if ((threadIdx.x & 31) == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
+}
+
+}  // namespace hz

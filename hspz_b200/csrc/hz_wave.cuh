@@ -341,328 +341,11 @@ __global__ void __launch_bounds__(kScopeThreads) scopes_kernel(WaveIn w, const u
   }
 }
 
-// ---------------------------------------------------------------------------
-// Gate: a persistent grid takes tiles of consecutive wave hits from a device
-// work queue.  Per tile it (1) recomputes the seeds of the positions
-// covering the tile and records the (position, seed) slots overlapping it,
-// (2) gives every hit its slot by a block max-scan of slot-start marks and
-// gathers its reference anchor from pos_table (coalesced within a slot), then
-// (3) runs the X-drop score gate thread-per-hit, all right extensions first
-// and all left extensions second, each lane refilling from the tile when its
-// extension ends, so extensions of different length do not idle the warp.
-// Eight cells are scored per step from two 4-byte words of each sequence.
-// Anchors are the END of the seed window on both sides (pos + seed_size,
-// src/gpu/kernels.rs:397-401).  A hit becomes a candidate when
-// (i32)(f32)(right max + left max) >= hspthresh -- the reference gate's bound
-// (src/gpu/kernels.rs:1048-1052), never below the final score since the
-// entropy factor is <= 1 -- or when an extension runs past `cap` cells
-// ("long"; the exact kernel redoes it warp-wide).
+}  // namespace hz
 
-// Slot records sit at the tile-relative index of their first hit, so a
-// max-scan of "first hit + 1" marks gives every hit its slot.
-template <int TILE>
-struct GateSmem {
-  int32_t sub[64];
-  uint32_t slot_bst[TILE];    // pos_table index of the slot's first in-tile hit
-  uint32_t slot_q[TILE];      // query anchor (absolute)
-  uint32_t slot_call[TILE];
-  uint32_t hit_slot[TILE];    // first hit of the hit's slot + 1 (mark, then max-scan)
-  uint32_t hit_r[TILE];       // reference anchor of each hit
-  int32_t hit_rmax[TILE];     // right-extension maximum, or kSpilled
-  uint16_t hit_rcells[TILE];  // right-extension cells (<= cap)
-  uint32_t warp_tot[kScanThreads / 32];
-  unsigned long long h0;
-  uint32_t next, e0, e1;
-};
-constexpr int32_t kSpilled = -1;  // a right maximum is never negative
+#include "hz_gate.cuh"
 
-struct GateArgs {
-  WaveIn w;
-  const unsigned long long *np_excl;
-  const uint32_t *np_pos;
-  const unsigned long long *scope_lo;
-  uint32_t scope_cap;  // entries of scope_lo (a wave with more scopes is rerun)
-  WaveTotals *tot;
-  int32_t sub[64];
-  int32_t xdrop;
-  int32_t hspthresh;
-  uint32_t cap;  // cells per direction before a hit goes to the exact kernel (multiple of 8)
-  Cand *cand;
-  uint32_t cand_cap;
-};
-
-__device__ __forceinline__ const uint32_t *word_ptr(const uint8_t *p) {
-  return reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)3);
-}
-
-// Inclusive max-scan of the slot marks over the tile.
-template <int TILE>
-__device__ __forceinline__ void mark_scan(GateSmem<TILE> &sm, uint32_t nt) {
-  constexpr int PER = TILE / kScanThreads;
-  uint32_t base = threadIdx.x * PER;
-  uint32_t run = 0;
-#pragma unroll
-  for (int i = 0; i < PER; i++)
-    if (base + i < nt) run = max(run, sm.hit_slot[base + i]);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint32_t incl = run;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl = max(incl, up);
-  }
-  if (lane == 31) sm.warp_tot[wid] = incl;
-  __syncthreads();
-  uint32_t carry = 0;
-  for (int i = 0; i < wid; i++) carry = max(carry, sm.warp_tot[i]);
-  uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
-  if (lane > 0) carry = max(carry, ex);
-#pragma unroll
-  for (int i = 0; i < PER; i++)
-    if (base + i < nt) {
-      carry = max(carry, sm.hit_slot[base + i]);
-      sm.hit_slot[base + i] = carry;
-    }
-}
-
-__device__ __forceinline__ uint32_t scope_of(const unsigned long long *scope_lo, uint32_t nscopes,
-                                             unsigned long long h) {
-  uint32_t lo = 0, hi = nscopes;  // last scope with scope_lo <= h
-  while (hi - lo > 1) {
-    uint32_t m = (lo + hi) >> 1;
-    if (scope_lo[m] <= h) lo = m; else hi = m;
-  }
-  return lo;
-}
-
-// Scores one cell whose byte offset into the substitution table is byte SH
-// of T; keeps every running sum S and maximum M for the termination path.
-#define HZ_CELL(T, SH, I)                                                            \
-  {                                                                                  \
-    int32_t sc = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH)) & 0xFFu)); \
-    S = (int32_t)((uint32_t)S + (uint32_t)sc);                                       \
-    M = max(M, S);                                                                   \
-    Si[I] = S;                                                                       \
-    Mi[I] = M;                                                                       \
-    D = max(D, (int32_t)((uint32_t)M - (uint32_t)S));                                \
-  }
-
-template <int TILE, bool LEFT>
-__device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm, uint32_t nt,
-                                           unsigned long long &cells_acc) {
-  const uint8_t *ref = a.w.ref;
-  const uint8_t *qbuf = a.w.qbuf;
-  const char *subb = reinterpret_cast<const char *>(sm.sub);
-  const int32_t X = a.xdrop;
-  const uint32_t lane = threadIdx.x & 31;
-  bool have = false, exhausted = false;
-  uint32_t t = 0, n = 0, r0 = 0, q0 = 0;
-  bool capped = false;
-  int32_t S = 0, M = 0;
-  uint32_t cells = 0;
-  const uint32_t *wr = nullptr, *wq = nullptr;
-  uint32_t cr = 0, cq = 0, sr = 0, sq = 0;
-  while (true) {
-    if (!exhausted) {
-      unsigned need = __ballot_sync(0xffffffffu, !have);
-      if (need) {
-        int leader = __ffs(need) - 1;
-        uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(&sm.next, (uint32_t)__popc(need));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (base + __popc(need) >= nt) exhausted = true;
-        if (!have) {
-          uint32_t mine = base + __popc(need & lanemask_lt());
-          if (mine < nt && !(LEFT && sm.hit_rmax[mine] == kSpilled)) {
-            have = true;
-            t = mine;
-            uint32_t slot = sm.hit_slot[t] - 1;
-            r0 = sm.hit_r[t];
-            q0 = sm.slot_q[slot];
-            const CallDev &cd = a.w.calls[sm.slot_call[slot]];
-            uint32_t qlo = cd.qoff;
-            if (!LEFT) n = min(a.w.rlen - r0, qlo + cd.qlen - q0);
-            else n = min(r0, q0 - qlo);
-            capped = n > a.cap;
-            if (capped) n = a.cap;
-            S = 0;
-            M = 0;
-            cells = 0;
-            sr = (r0 & 3u) * 8u;
-            sq = (q0 & 3u) * 8u;
-            if (!LEFT) {
-              wr = word_ptr(ref + r0);
-              wq = word_ptr(qbuf + q0);
-              cr = __ldg(wr);
-              cq = __ldg(wq);
-            } else {
-              wr = word_ptr(ref + r0 - 8);
-              wq = word_ptr(qbuf + q0 - 8);
-              cr = __ldg(wr + 2);
-              cq = __ldg(wq + 2);
-            }
-          }
-        }
-      }
-    }
-    // (in the left pass a refill may hand out only hits that were spilled in
-    // the right pass, so an idle warp ends only once the tile is exhausted)
-    if (!__any_sync(0xffffffffu, have) && exhausted) break;
-    if (!have) continue;
-    // ---- eight cells ----
-    uint32_t ra, rb, qa, qb;
-    if (!LEFT) {
-      uint32_t rm = __ldg(wr + 1), rh = __ldg(wr + 2);
-      uint32_t qm = __ldg(wq + 1), qh = __ldg(wq + 2);
-      ra = __funnelshift_r(cr, rm, sr);
-      rb = __funnelshift_r(rm, rh, sr);
-      qa = __funnelshift_r(cq, qm, sq);
-      qb = __funnelshift_r(qm, qh, sq);
-      cr = rh;
-      cq = qh;
-      wr += 2;
-      wq += 2;
-    } else {
-      uint32_t rm = __ldg(wr + 1), rl = __ldg(wr);
-      uint32_t qm = __ldg(wq + 1), ql = __ldg(wq);
-      ra = __byte_perm(__funnelshift_r(rm, cr, sr), 0, 0x0123);
-      rb = __byte_perm(__funnelshift_r(rl, rm, sr), 0, 0x0123);
-      qa = __byte_perm(__funnelshift_r(qm, cq, sq), 0, 0x0123);
-      qb = __byte_perm(__funnelshift_r(ql, qm, sq), 0, 0x0123);
-      cr = rl;
-      cq = ql;
-      wr -= 2;
-      wq -= 2;
-    }
-    // codes are 0..7, so (r << 5) | (q << 2) is the byte offset of sub[r*8+q]
-    uint32_t ta = (ra << 5) | (qa << 2), tb = (rb << 5) | (qb << 2);
-    const int32_t Ms = M;
-    int32_t Si[8], Mi[8];
-    int32_t D = 0;
-    HZ_CELL(ta, 0, 0)
-    HZ_CELL(ta, 8, 1)
-    HZ_CELL(ta, 16, 2)
-    HZ_CELL(ta, 24, 3)
-    HZ_CELL(tb, 0, 4)
-    HZ_CELL(tb, 8, 5)
-    HZ_CELL(tb, 16, 6)
-    HZ_CELL(tb, 24, 7)
-    if (D <= X && n > 8) {  // no drop and more cells left
-      n -= 8;
-      cells += 8;
-      continue;
-    }
-    // The extension ends in this group: at the first valid cell with
-    // M - S > xdrop (keeping the maximum from before it), or after the v
-    // valid cells left before the edge or the cap.
-    uint32_t v = min(n, 8u);
-    uint32_t dm = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
-    dm &= (1u << v) - 1u;
-    uint32_t stop = dm ? (uint32_t)(__ffs(dm) - 1) : v;
-    int32_t res = Ms;
-#pragma unroll
-    for (int i = 1; i <= 8; i++)
-      if ((uint32_t)i == stop) res = Mi[i - 1];
-    cells += dm ? stop + 1 : v;
-    const bool spill = !dm && capped;
-    if (spill) {
-      uint32_t at = atomicAdd(&a.tot->cand, 1u);
-      if (at < a.cand_cap) {
-        uint32_t slot = sm.hit_slot[t] - 1;
-        a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), r0, q0,
-                             sm.slot_call[slot] | kLongFlag};
-      }
-      if (!LEFT) sm.hit_rmax[t] = kSpilled;  // the left pass skips it
-    } else if (!LEFT) {
-      sm.hit_rmax[t] = res;
-      sm.hit_rcells[t] = (uint16_t)cells;
-    } else {
-      cells_acc += cells + sm.hit_rcells[t];
-      int32_t total = (int32_t)((uint32_t)sm.hit_rmax[t] + (uint32_t)res);
-      if (sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
-        uint32_t at = atomicAdd(&a.tot->cand, 1u);
-        if (at < a.cand_cap) {
-          uint32_t slot = sm.hit_slot[t] - 1;
-          a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), r0, q0,
-                             sm.slot_call[slot]};
-        }
-      }
-    }
-    have = false;
-  }
-}
-
-template <int TILE>
-__global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
-  static_assert(TILE % kScanThreads == 0, "tile must be a multiple of the block");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  GateSmem<TILE> &sm = *reinterpret_cast<GateSmem<TILE> *>(smem_raw);
-  if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
-  unsigned long long cells_acc = 0;
-  const unsigned long long total = a.tot->hits;
-  const uint32_t nz = a.tot->nz;
-  const WaveIn &w = a.w;
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) sm.h0 = atomicAdd(&a.tot->tiles, 1ull) * (unsigned long long)TILE;
-    __syncthreads();
-    const unsigned long long h0 = sm.h0;
-    if (h0 >= total) break;
-    const uint32_t nt = (uint32_t)min((unsigned long long)TILE, total - h0);
-    // positions covering [h0, h0 + nt)
-    if (threadIdx.x < 2) {
-      unsigned long long h = threadIdx.x == 0 ? h0 : h0 + nt - 1;
-      uint32_t k = last_le(a.np_excl, 0, nz, h);
-      if (threadIdx.x == 0) sm.e0 = k; else sm.e1 = k;
-    }
-    if (threadIdx.x == 0) sm.next = 0;
-    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) sm.hit_slot[i] = 0;
-    __syncthreads();
-    // (1) slots overlapping the tile
-    const uint32_t e0 = sm.e0, e1 = sm.e1;
-    for (uint32_t k = e0 + threadIdx.x; k <= e1; k += blockDim.x) {
-      uint32_t p = a.np_pos[k];
-      uint32_t c = call_of(w.calls, w.ncalls, p);
-      CallDev cd = w.calls[c];
-      uint32_t qpos, kmer;
-      position_seed(w, cd, p, &qpos, &kmer);
-      unsigned long long lo = a.np_excl[k];
-      for (uint32_t v = 0; v < w.per_pos; v++) {
-        uint32_t beg;
-        uint32_t cnt = bucket(w, seed_variant(kmer, v), &beg);
-        unsigned long long hi = lo + cnt;
-        if (cnt && hi > h0 && lo < h0 + nt) {
-          unsigned long long first = lo > h0 ? lo : h0;
-          uint32_t s = (uint32_t)(first - h0);
-          sm.slot_bst[s] = beg + (uint32_t)(first - lo);
-          sm.slot_q[s] = cd.qoff + qpos + w.shape.size;
-          sm.slot_call[s] = c;
-          sm.hit_slot[s] = s + 1;
-        }
-        lo = hi;
-      }
-    }
-    __syncthreads();
-    // (2) hit -> slot, reference anchor
-    mark_scan<TILE>(sm, nt);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-      uint32_t s = sm.hit_slot[i] - 1;
-      sm.hit_r[i] = __ldg(w.pos_table + sm.slot_bst[s] + (i - s)) + w.shape.size;
-    }
-    __syncthreads();
-    // (3) the score gate
-    gate_phase<TILE, false>(a, sm, nt, cells_acc);
-    __syncthreads();
-    if (threadIdx.x == 0) sm.next = 0;
-    __syncthreads();
-    gate_phase<TILE, true>(a, sm, nt, cells_acc);
-  }
-  for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
-  if ((threadIdx.x & 31) == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
-}
+namespace hz {
 
 // ---------------------------------------------------------------------------
 // Exact extension, one warp per candidate: the reference's warp mapping of

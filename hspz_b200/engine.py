@@ -172,6 +172,11 @@ class Engine:
         N.check(N.lib().hz_stage_queries(self._h, qs, len(arrs)))
         self._staged = arrs  # keep alive until the copies are done (they are synchronous)
 
+    def select_query(self, index: int):
+        """Point the per-call entry points (run_pass, seed_and_filter, ...) at
+        staged query `index` without uploading it again."""
+        N.check(N.lib().hz_select_query(self._h, index))
+
     def run_batched(self):
         """Every call of every staged query through shared waves; records per
         query in the same order run_pass gives for that query alone."""

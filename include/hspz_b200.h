@@ -148,6 +148,11 @@ typedef struct hz_batch_record {
  * resident).  Both strands are encoded on the device. */
 int hz_stage_queries(hz_engine *e, const hz_query *queries, uint32_t nq);
 
+/* Makes staged query `index` the one that swap_query would have put in place
+ * (the target of hz_generate_seeds / hz_upload_seeds / hz_seed_and_filter /
+ * hz_run_pass), without another upload. */
+int hz_select_query(hz_engine *e, uint32_t index);
+
 /* Batched form of seed_and_filter_all (src/run.rs:266-495) over every staged
  * query: all calls of many queries go through shared waves (one lookup, one
  * persistent gate launch over a device work queue, one read-back per wave)
@@ -169,7 +174,7 @@ int hz_engine_profile_entry(hz_engine *e, uint32_t i, char *name, uint32_t name_
 int hz_engine_profile_reset(hz_engine *e);
 
 /* Launch-shape knobs (no reference counterpart; results never depend on
- * them): "gate_tile" (hits per gate block tile: 1024, 2048, 4096),
+ * them): "gate_tile" (hits per gate block tile: 512, 768, 1024, 2048, 4096),
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
  * "wave_positions" (seed positions per batched wave). */
