@@ -260,7 +260,8 @@ struct hz_engine {
   Slot slot[2];
   // wave buffers
   DBuf<CallDev> calls;
-  DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope;
+  DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope, tile_first;
+  uint32_t tile_cap = 1u << 16;  // entries of the gate's tile table
   DBuf<unsigned long long> np_excl, call_hit_lo, scope_lo;
   DBuf<HitNz> np_partial, np_grand;
   DBuf<WaveTotals> tot;
@@ -426,6 +427,11 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
           np_totals_kernel<<<1, 32, 0, s>>>(e->np_grand.p, e->tot.p, e->np_excl.p);
         },
         4));
+    TRY(e->tile_first.ensure(e->tile_cap, s));
+    TRY(e->launch("tile_table", [&] {
+      tile_table_kernel<<<grid_for(npos, 256, e->sm_count * 8), 256, 0, s>>>(
+          e->np_excl.p, e->pos_hits.p, e->np_pos.p, e->tot.p, (uint32_t)e->gate_tile, e->tile_first.p, e->tile_cap);
+    }));
     TRY(e->launch("scopes", [&] {
       scopes_kernel<<<1, kScopeThreads, 0, s>>>(w, e->np_excl.p, e->np_pos.p, e->tot.p, e->max_hits,
                                                 e->call_hit_lo.p, e->call_nz_lo.p, e->scope_lo.p, e->scope_call.p,
@@ -444,6 +450,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     ga.cap = e->gate_cap;
     ga.cand = e->cand.p;
     ga.cand_cap = e->cand_cap;
+    ga.tile_first = e->tile_first.p;
     switch (e->gate_tile) {
       case 512: TRY(launch_gate<512>(e, ga)); break;
       case 768: TRY(launch_gate<768>(e, ga)); break;
@@ -477,6 +484,10 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       return fail(HZ_E_INVALID, "the first seed of a call holds more than max_hits=%u hits; the reference's MAX_HITS "
                                 "walk has no valid cut there", e->max_hits);
     bool again = false;
+    if (t.status & 4u) {  // the gate skipped the wave: its tile table was too small
+      e->tile_cap = (uint32_t)std::min<uint64_t>(t.hits / (uint64_t)e->gate_tile + 1024, 0xFFFFFFF0ull);
+      again = true;
+    }
     if (t.n_scopes > scope_cap) {
       e->scope_cap = t.n_scopes + 16;
       again = true;

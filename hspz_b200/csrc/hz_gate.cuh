@@ -50,7 +50,8 @@ struct GateSmem {
   uint16_t hit_rcells[TILE];
   uint32_t warp_tot[kScanThreads / 32];
   unsigned long long h0;
-  uint32_t next, e0, e1;
+  uint32_t next, e0, e1, c0;
+  uint32_t next_w[kScanThreads / 32];
 };
 constexpr int32_t kSpilled = -1;  // a right maximum is never negative
 
@@ -67,6 +68,7 @@ struct GateArgs {
   uint32_t cap;  // cells per direction before a hit goes to the exact kernel (multiple of 8, < 65536)
   Cand *cand;
   uint32_t cand_cap;
+  const uint32_t *tile_first;  // first position with hits of each tile (tile_table_kernel)
 };
 
 __device__ __forceinline__ const uint32_t *word_ptr(const uint8_t *p) {
@@ -137,7 +139,8 @@ __device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint
 
 // Scores one cell whose byte offset into the substitution table is byte SH
 // of T; keeps every running sum S and maximum M for the termination path
-// and the group's largest M - S in D.
+// and the group's smallest sum. Since every M_i <= M_7, no cell of the group
+// can have dropped when M_7 - min S <= xdrop.
 #define HZ_CELL(T, SH, I)                                                            \
   {                                                                                  \
     int32_t sc = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH)) & 0xFFu)); \
@@ -145,12 +148,12 @@ __device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint
     M = max(M, S);                                                                   \
     Si[I] = S;                                                                       \
     Mi[I] = M;                                                                       \
-    D = max(D, (int32_t)((uint32_t)M - (uint32_t)S));                                \
+    Smin = min(Smin, S);                                                             \
   }
 
 template <int TILE, bool LEFT>
-__device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm, uint32_t nt,
-                                           unsigned long long &cells_acc) {
+__device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm, uint32_t lo, uint32_t hi,
+                                           uint32_t *ctr, unsigned long long &cells_acc) {
   const uint8_t *ref = a.w.ref;
   const uint8_t *qbuf = a.w.qbuf;
   const char *subb = reinterpret_cast<const char *>(sm.sub);
@@ -172,12 +175,12 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
       if (need) {
         int leader = __ffs(need) - 1;
         uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(&sm.next, (uint32_t)__popc(need));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (base + __popc(need) >= nt) exhausted = true;
+        if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(need));
+        base = lo + __shfl_sync(0xffffffffu, base, leader);
+        if (base + __popc(need) >= hi) exhausted = true;
         if (!have) {
           uint32_t mine = base + __popc(need & lanemask_lt());
-          if (mine < nt && !(LEFT && sm.hit_rmax[mine] == kSpilled)) {
+          if (mine < hi && !(LEFT && sm.hit_rmax[mine] == kSpilled)) {
             have = true;
             t = mine;
             const uint32_t r0 = sm.hit_r[t], q0 = sm.hit_q[t];
@@ -246,7 +249,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
     }
     const int32_t Ms = M;
     int32_t Si[8], Mi[8];
-    int32_t D = 0;
+    int32_t Smin = S;
     HZ_CELL(ta, 0, 0)
     HZ_CELL(ta, 8, 1)
     HZ_CELL(ta, 16, 2)
@@ -255,7 +258,15 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
     HZ_CELL(tb, 8, 5)
     HZ_CELL(tb, 16, 6)
     HZ_CELL(tb, 24, 7)
-    if (D <= X && n > 8) {  // no drop and more cells left: advance the stream
+    // first valid cell with M - S > xdrop, if the bound says there may be one
+    const uint32_t v = min(n, 8u);
+    uint32_t dm = 0;
+    if ((int32_t)((uint32_t)M - (uint32_t)Smin) > X || n <= 8) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
+      dm &= (1u << v) - 1u;
+    }
+    if (!dm && n > 8) {  // no drop and more cells left: advance the stream
       n -= 8;
       cells += 8;
       ra = nra;
@@ -280,11 +291,6 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
     // The extension ends in this group: at the first valid cell with
     // M - S > xdrop (keeping the maximum from before it), or after the v
     // valid cells left before the edge or the cap.
-    const uint32_t v = min(n, 8u);
-    uint32_t dm = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
-    dm &= (1u << v) - 1u;
     const uint32_t stop = dm ? (uint32_t)(__ffs(dm) - 1) : v;
     int32_t res = Ms;
 #pragma unroll
@@ -317,8 +323,9 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
 
 // Fills the first eight cells and the carried word of every hit for one pass.
 template <int TILE, bool LEFT>
-__device__ __forceinline__ void prepare_pass(const GateArgs &a, GateSmem<TILE> &sm, uint32_t nt) {
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+__device__ __forceinline__ void prepare_pass(const GateArgs &a, GateSmem<TILE> &sm, uint32_t lo, uint32_t hi,
+                                             uint32_t first_thread, uint32_t nthreads) {
+  for (uint32_t i = lo + first_thread; i < hi; i += nthreads) {
     if (LEFT && sm.hit_rmax[i] == kSpilled) continue;
     uint32_t ra, rb, rc, qa, qb, qc;
     first_group<LEFT>(a.w.ref, sm.hit_r[i], &ra, &rb, &rc);
@@ -333,6 +340,7 @@ __global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
   static_assert(TILE % kScanThreads == 0, "tile must be a multiple of the block");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   GateSmem<TILE> &sm = *reinterpret_cast<GateSmem<TILE> *>(smem_raw);
+  if (a.tot->status & 4u) return;  // no tile table: the host reruns the wave with a larger one
   if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
   unsigned long long cells_acc = 0;
   const unsigned long long total = a.tot->hits;
@@ -345,20 +353,25 @@ __global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
     const unsigned long long h0 = sm.h0;
     if (h0 >= total) break;
     const uint32_t nt = (uint32_t)min((unsigned long long)TILE, total - h0);
-    // positions covering [h0, h0 + nt)
-    if (threadIdx.x < 2) {
-      unsigned long long h = threadIdx.x == 0 ? h0 : h0 + nt - 1;
-      uint32_t k = last_le(a.np_excl, 0, nz, h);
-      if (threadIdx.x == 0) sm.e0 = k; else sm.e1 = k;
+    // positions covering [h0, h0 + nt): the tile table gives the first; the
+    // last is the one before the next tile's first, unless that one already
+    // started inside this tile
+    if (threadIdx.x == 0) {
+      const uint32_t j = (uint32_t)(h0 / TILE);
+      const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
+      sm.e0 = k0;
+      sm.e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
+      sm.c0 = call_of(w.calls, w.ncalls, a.np_pos[k0]);
+      sm.next = 0;
     }
-    if (threadIdx.x == 0) sm.next = 0;
     for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) sm.u.setup.hit_slot[i] = 0;
     __syncthreads();
     // (1) slots overlapping the tile
     const uint32_t e0 = sm.e0, e1 = sm.e1;
+    uint32_t c = sm.c0;  // calls only advance with the position
     for (uint32_t k = e0 + threadIdx.x; k <= e1; k += blockDim.x) {
       uint32_t p = a.np_pos[k];
-      uint32_t c = call_of(w.calls, w.ncalls, p);
+      while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
       CallDev cd = w.calls[c];
       uint32_t qpos, kmer;
       position_seed(w, cd, p, &qpos, &kmer);
@@ -397,14 +410,30 @@ __global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
     }
     __syncthreads();
     // (3) the score gate: right pass, then left pass
-    prepare_pass<TILE, false>(a, sm, nt);
+    prepare_pass<TILE, false>(a, sm, 0, nt, threadIdx.x, blockDim.x);
     __syncthreads();
-    gate_phase<TILE, false>(a, sm, nt, cells_acc);
+#ifdef HZ_GATE_WARP_SLICES
+    {
+      // each warp takes a fixed slice of the tile through both passes
+      const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      const uint32_t lo = (uint32_t)((uint64_t)nt * wid / nw), hi = (uint32_t)((uint64_t)nt * (wid + 1) / nw);
+      if (lane == 0) sm.next_w[wid] = 0;
+      __syncwarp();
+      gate_phase<TILE, false>(a, sm, lo, hi, &sm.next_w[wid], cells_acc);
+      __syncwarp();
+      if (lane == 0) sm.next_w[wid] = 0;
+      prepare_pass<TILE, true>(a, sm, lo, hi, lane, 32);
+      __syncwarp();
+      gate_phase<TILE, true>(a, sm, lo, hi, &sm.next_w[wid], cells_acc);
+    }
+#else
+    gate_phase<TILE, false>(a, sm, 0, nt, &sm.next, cells_acc);
     __syncthreads();
     if (threadIdx.x == 0) sm.next = 0;
-    prepare_pass<TILE, true>(a, sm, nt);
+    prepare_pass<TILE, true>(a, sm, 0, nt, threadIdx.x, blockDim.x);
     __syncthreads();
-    gate_phase<TILE, true>(a, sm, nt, cells_acc);
+    gate_phase<TILE, true>(a, sm, 0, nt, &sm.next, cells_acc);
+#endif
   }
   for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
   if ((threadIdx.x & 31) == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);

@@ -201,6 +201,29 @@ __global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *_
   }
 }
 
+// The gate's tile table: tile_first[j] = the position with hits that holds
+// wave hit j * tile (positions tile the hit space, so every tile start has
+// exactly one), and tile_first[n_tiles] = nz.  Lets a gate block find its
+// positions with two loads instead of a search.  Sets status bit 2 when the
+// table is too small (the wave is then rerun with a larger one).
+__global__ void tile_table_kernel(const unsigned long long *__restrict__ np_excl, const uint32_t *__restrict__ pos_hits,
+                                  const uint32_t *__restrict__ np_pos, WaveTotals *__restrict__ t, uint32_t tile,
+                                  uint32_t *__restrict__ tile_first, uint32_t cap) {
+  const uint32_t nz = t->nz;
+  const unsigned long long total = t->hits;
+  const unsigned long long n_tiles = (total + tile - 1) / tile;
+  if (n_tiles + 1 > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&t->status, 4u);
+    return;
+  }
+  uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nz; k += stride) {
+    unsigned long long lo = np_excl[k], hi = lo + pos_hits[np_pos[k]];
+    for (unsigned long long j = (lo + tile - 1) / tile; j * tile < hi; j++) tile_first[j] = k;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) tile_first[n_tiles] = nz;
+}
+
 // Grand totals of the scan into WaveTotals, and the sentinel np_excl[nz].
 __global__ void np_totals_kernel(const HitNz *__restrict__ grand, WaveTotals *__restrict__ t,
                                  unsigned long long *__restrict__ np_excl) {
