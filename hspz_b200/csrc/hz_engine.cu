@@ -20,6 +20,7 @@
 #include "hz_kernels.cuh"
 #include "hz_scan.cuh"
 #include "hz_wave.cuh"
+#include "hz_dedup.cuh"
 
 using namespace hz;
 
@@ -271,6 +272,11 @@ struct hz_engine {
   HBuf<WaveTotals> h_tot;
   HBuf<hz_segment_pair> h_raw;
   HBuf<uint32_t> h_raw_scope, h_scope_call;
+  // device dedup of the batched form
+  bool device_dedup = true;
+  DBuf<uint32_t> d_perm_a, d_perm_b, d_keys_a, d_keys_b, d_keep, d_keep_excl, d_hist, d_hpart, d_total;
+  DBuf<ScopedHspOut> d_out;
+  HBuf<ScopedHspOut> h_out;
   uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
   // tuning
   int gate_tile = 1024;
@@ -360,8 +366,82 @@ template <int TILE> int launch_gate(hz_engine *e, const GateArgs &ga) {
 // Runs calls[0..n) as one wave and appends its deduped HSPs, in call order
 // and LASTZ order within each MAX_HITS scope, to *out.  `seeds` (device) is
 // the uploaded seed array of a single-call wave, or null.
+// dedup_and_order of every scope of a wave on the device (hz_dedup.cuh);
+// appends the kept HSPs, in scope order and LASTZ order within each scope.
+int dedup_on_device(hz_engine *e, uint32_t nraw, uint32_t n_scopes, std::vector<WaveRecord> *out, hz_stats *st) {
+  cudaStream_t s = e->st;
+  TRY(e->d_perm_a.ensure(nraw, s));
+  TRY(e->d_perm_b.ensure(nraw, s));
+  TRY(e->d_keys_a.ensure(nraw, s));
+  TRY(e->d_keys_b.ensure(nraw, s));
+  TRY(e->d_keep.ensure(nraw, s));
+  TRY(e->d_keep_excl.ensure(nraw, s));
+  uint64_t rtiles = (nraw + kRadixTile - 1) / kRadixTile;
+  TRY(e->d_hist.ensure(rtiles * kRadixBins, s));
+  TRY(e->d_hpart.ensure(scan_tiles(std::max<uint64_t>(rtiles * kRadixBins, nraw)) + 1, s));
+  TRY(e->d_total.ensure(1, s));
+  const unsigned g = grid_for(nraw, 256);
+  TRY(e->launch("dedup", [&] { iota_kernel<<<g, 256, 0, s>>>(e->d_perm_a.p, nraw); }));
+  uint32_t scope_bytes = 1;
+  while (scope_bytes < 4 && (n_scopes >> (8 * scope_bytes))) scope_bytes++;
+  // stable LSD passes over the fields of a key, least significant first
+  auto sort_by = [&](const int *fields, int nf, uint32_t cnt) -> int {
+    uint64_t tiles = (cnt + kRadixTile - 1) / kRadixTile;
+    for (int fi = 0; fi < nf; fi++) {
+      int f = fields[fi];
+      TRY(e->launch("dedup", [&] {
+        gather_key_kernel<<<grid_for(cnt, 256), 256, 0, s>>>(e->raw.p, e->raw_scope.p, e->d_perm_a.p, cnt, f,
+                                                            e->d_keys_a.p);
+      }));
+      int passes = f == kScope ? (int)scope_bytes : 4;
+      for (int p = 0; p < passes; p++) {
+        int shift = 8 * p;
+        TRY(e->launch("dedup", [&] {
+          radix_hist_kernel<<<(unsigned)tiles, kRadixThreads, 0, s>>>(e->d_keys_a.p, cnt, shift, e->d_hist.p, tiles);
+          exclusive_scan<uint32_t>(e->d_hist.p, e->d_hist.p, tiles * kRadixBins, e->d_hpart.p, e->d_total.p, s);
+          radix_scatter_kernel<<<(unsigned)tiles, kRadixThreads, 0, s>>>(e->d_keys_a.p, e->d_perm_a.p, cnt, shift,
+                                                                        e->d_hist.p, tiles, e->d_keys_b.p,
+                                                                        e->d_perm_b.p);
+        }, 5));
+        std::swap(e->d_keys_a, e->d_keys_b);
+        std::swap(e->d_perm_a, e->d_perm_b);
+      }
+    }
+    return HZ_OK;
+  };
+  static const int by_diagonal_key[5] = {kScoreDesc, kLen, kRefStart, kDiag, kScope};
+  static const int by_lastz_key[5] = {kScoreDesc, kLen, kRefStart, kQueryStart, kScope};
+  TRY(sort_by(by_diagonal_key, 5, nraw));
+  TRY(e->launch("dedup", [&] {
+    keep_flag_kernel<<<g, 256, 0, s>>>(e->raw.p, e->raw_scope.p, e->d_perm_a.p, nraw, e->d_keep.p);
+    exclusive_scan<uint32_t>(e->d_keep.p, e->d_keep_excl.p, nraw, e->d_hpart.p, e->d_total.p, s);
+    compact_perm_kernel<<<g, 256, 0, s>>>(e->d_perm_a.p, e->d_keep_excl.p, e->d_keep.p, nraw, e->d_perm_b.p);
+  }, 5));
+  uint32_t kept = 0;
+  CK(cudaMemcpyAsync(&kept, e->d_total.p, 4, cudaMemcpyDeviceToHost, s));
+  TRY(e->sync());
+  std::swap(e->d_perm_a, e->d_perm_b);
+  TRY(sort_by(by_lastz_key, 5, kept));
+  TRY(e->d_out.ensure(kept + 1, s));
+  TRY(e->h_out.ensure(kept + 1));
+  TRY(e->h_scope_call.ensure(n_scopes + 1));
+  TRY(e->launch("dedup", [&] {
+    emit_scoped_kernel<<<grid_for(kept, 256), 256, 0, s>>>(e->raw.p, e->raw_scope.p, e->d_perm_a.p, kept, e->d_out.p);
+  }));
+  CK(cudaMemcpyAsync(e->h_out.p, e->d_out.p, (size_t)kept * sizeof(ScopedHspOut), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(e->h_scope_call.p, e->scope_call.p, (size_t)n_scopes * 4, cudaMemcpyDeviceToHost, s));
+  TRY(e->sync());
+  for (uint32_t i = 0; i < kept; i++) {
+    const ScopedHspOut &r = e->h_out.p[i];
+    out->push_back(WaveRecord{e->h_scope_call.p[r.scope],
+                              hz_segment_pair{r.h.ref_start, r.h.query_start, r.h.len, r.h.score}});
+  }
+  if (st) st->hsps += kept;
+  return HZ_OK;
+}
+
 int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, int transitions,
-             std::vector<WaveRecord> *out, hz_stats *st) {
+             std::vector<WaveRecord> *out, hz_stats *st, bool device_dedup) {
   if (n == 0) return HZ_OK;
   cudaStream_t s = e->st;
   uint64_t npos = 0;
@@ -512,6 +592,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       st->calls += n;
     }
     if (nraw == 0) return HZ_OK;
+    if (device_dedup) return dedup_on_device(e, nraw, t.n_scopes, out, st);
     TRY(e->h_raw.ensure(nraw));
     TRY(e->h_raw_scope.ensure(nraw));
     TRY(e->h_scope_call.ensure(t.n_scopes + 1));
@@ -727,6 +808,11 @@ void hz_engine_destroy(hz_engine *e) {
   e->h_raw.release();
   e->h_raw_scope.release();
   e->h_scope_call.release();
+  for (auto *b : {&e->d_perm_a, &e->d_perm_b, &e->d_keys_a, &e->d_keys_b, &e->d_keep, &e->d_keep_excl, &e->d_hist,
+                  &e->d_hpart, &e->d_total, &e->tile_first})
+    b->release();
+  e->d_out.release();
+  e->h_out.release();
   for (auto &pe : e->pending) {
     cudaEventDestroy(pe.second.first);
     cudaEventDestroy(pe.second.second);
@@ -1020,10 +1106,10 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
   std::vector<WaveRecord> recs;
   if (s.kind == 2) {
     HostCall hc{e->cur_query, 0, (uint32_t)(rev ? 1 : 0), s.start, s.end};
-    TRY(run_wave(e, &hc, s.end > s.start ? 1 : 0, nullptr, s.transitions, &recs, &local));
+    TRY(run_wave(e, &hc, s.end > s.start ? 1 : 0, nullptr, s.transitions, &recs, &local, false));
   } else if (s.n) {
     HostCall hc{e->cur_query, 0, (uint32_t)(rev ? 1 : 0), 0, (uint32_t)s.n};
-    TRY(run_wave(e, &hc, 1, s.seeds.p, 0, &recs, &local));
+    TRY(run_wave(e, &hc, 1, s.seeds.p, 0, &recs, &local, false));
   }
   local.seeds = s.n;
   TRY(copy_out_segments(recs, out, n));
@@ -1047,7 +1133,7 @@ int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats
   std::vector<WaveRecord> recs;
   for (size_t i = 0; i < calls.size(); i++) {
     size_t before = recs.size();
-    TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local));
+    TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local, false));
     for (size_t k = before; k < recs.size(); k++) recs[k].call = (uint32_t)i;  // wave-relative -> pass call
   }
   // records of one interval: plus calls before minus calls (call order already)
@@ -1107,7 +1193,7 @@ int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *s
       j++;
     }
     size_t before = recs.size();
-    TRY(run_wave(e, calls.data() + i, j - i, nullptr, e->cfg.transitions, &recs, &local));
+    TRY(run_wave(e, calls.data() + i, j - i, nullptr, e->cfg.transitions, &recs, &local, e->device_dedup));
     for (size_t k = before; k < recs.size(); k++) recs[k].call += (uint32_t)i;
     i = j;
   }
@@ -1174,6 +1260,8 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   } else if (k == "gate_blocks_per_sm") {
     if (value < 0 || value > 32) return fail(HZ_E_INVALID, "gate_blocks_per_sm must be 0..32");
     e->gate_blocks_per_sm = (int)value;
+  } else if (k == "device_dedup") {
+    e->device_dedup = value != 0;
   } else if (k == "wave_positions") {
     if (value < 1 || value >= (1ll << 31)) return fail(HZ_E_INVALID, "wave_positions must be 1..2^31-1");
     e->wave_positions = (uint64_t)value;

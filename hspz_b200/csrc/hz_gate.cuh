@@ -412,7 +412,6 @@ __global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
     // (3) the score gate: right pass, then left pass
     prepare_pass<TILE, false>(a, sm, 0, nt, threadIdx.x, blockDim.x);
     __syncthreads();
-#ifdef HZ_GATE_WARP_SLICES
     {
       // each warp takes a fixed slice of the tile through both passes
       const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -426,14 +425,6 @@ __global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
       __syncwarp();
       gate_phase<TILE, true>(a, sm, lo, hi, &sm.next_w[wid], cells_acc);
     }
-#else
-    gate_phase<TILE, false>(a, sm, 0, nt, &sm.next, cells_acc);
-    __syncthreads();
-    if (threadIdx.x == 0) sm.next = 0;
-    prepare_pass<TILE, true>(a, sm, 0, nt, threadIdx.x, blockDim.x);
-    __syncthreads();
-    gate_phase<TILE, true>(a, sm, 0, nt, &sm.next, cells_acc);
-#endif
   }
   for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
   if ((threadIdx.x & 31) == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);

@@ -177,7 +177,8 @@ int hz_engine_profile_reset(hz_engine *e);
  * them): "gate_tile" (hits per gate block tile: 512, 768, 1024, 2048, 4096),
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
- * "wave_positions" (seed positions per batched wave). */
+ * "wave_positions" (seed positions per batched wave), "device_dedup" (1: the
+ * batched form dedups on the device, 0: on the host as the plain form does). */
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
 
 /* Kernel launches issued by this engine since creation. */

@@ -58,7 +58,9 @@ def test_batched_equals_plain_per_query(workload):
 
 
 @pytest.mark.parametrize("tuning", [dict(wave_positions=50_000), dict(gate_cap=8), dict(gate_cap=4096),
-                                    dict(gate_tile=1024, gate_blocks_per_sm=1), dict(gate_tile=4096)])
+                                    dict(gate_tile=1024, gate_blocks_per_sm=1), dict(gate_tile=4096),
+                                    dict(gate_tile=512), dict(device_dedup=0),
+                                    dict(device_dedup=0, wave_positions=5_000)])
 def test_launch_shapes_do_not_change_results(workload, tuning):
     target, chunks = workload
     chunks = chunks[:16]
