@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1207,6 +1208,160 @@ int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *s
   }
   *n = recs.size();
   if (stats) *stats = local;
+  return HZ_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dedup_and_order of HSPs that already sit in device memory, without
+// allocating anything.  Some callers cannot allocate device memory: a host
+// program whose own allocator owns the whole device, a serving loop that
+// admits work against a fixed memory budget, or a plugin that must not grow
+// the process's footprint behind its host's back.  For them this entry point
+// runs the batched form's device dedup (radix passes, containment, LASTZ
+// order) on a fixed scratch array compiled into this library instead of on
+// engine buffers.
+
+namespace {
+
+constexpr uint32_t kNoAllocMax = HZ_NOALLOC_MAX_HSPS;
+constexpr uint32_t kNoAllocTiles = (kNoAllocMax + kRadixTile - 1) / kRadixTile;
+constexpr uint32_t kNoAllocHist = kNoAllocTiles * kRadixBins;
+constexpr uint32_t kNoAllocPartials = kNoAllocHist / kScanTile + 2;
+// u32 words: perm_a, perm_b, keys_a, keys_b, dropped flags (kNoAllocMax each),
+// radix histograms, scan partials, scan total, kept count
+constexpr size_t kNoAllocWords = 5ull * kNoAllocMax + kNoAllocHist + kNoAllocPartials + 2;
+
+}  // namespace
+
+// The scratch: ~6 MB that every GPU which loads this library holds until the
+// process exits.  Shared by every call; it keeps the last call's contents.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+namespace {
+
+// Unaligned-tolerant view of hz_segment_pair (the caller's buffers need only
+// 4-byte alignment).
+struct PlainHsp {
+  uint32_t ref_start, query_start, len;
+  int32_t score;
+};
+
+constexpr int kDroppedField = 6;
+
+__global__ void na_gather_kernel(const PlainHsp *__restrict__ in, const uint32_t *__restrict__ perm,
+                                 const uint32_t *__restrict__ dropped, uint32_t n, int field,
+                                 uint32_t *__restrict__ keys) {
+  uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t r = perm[i];
+    if (field == kDroppedField) {
+      keys[i] = dropped[r];
+      continue;
+    }
+    SegmentPair h{in[r].ref_start, in[r].query_start, in[r].len, in[r].score};
+    keys[i] = field_key(h, 0u, field);
+  }
+}
+
+// After the hspComp sort: a record is dropped when it is contained in the
+// previous input record (src/hsp.rs:94-126); kept ones are counted.
+__global__ void na_flag_kernel(const PlainHsp *__restrict__ in, const uint32_t *__restrict__ perm, uint32_t n,
+                               uint32_t *__restrict__ dropped, uint32_t *__restrict__ kept) {
+  uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t r = perm[i];
+    bool d = false;
+    if (i > 0) {
+      const PlainHsp &a = in[perm[i - 1]], &b = in[r];
+      d = contained_dev(SegmentPair{a.ref_start, a.query_start, a.len, a.score},
+                        SegmentPair{b.ref_start, b.query_start, b.len, b.score});
+    }
+    dropped[r] = d;
+    if (!d) atomicAdd(kept, 1u);
+  }
+}
+
+__global__ void na_copy_kernel(const PlainHsp *__restrict__ in, const uint32_t *__restrict__ perm,
+                               const uint32_t *__restrict__ kept, PlainHsp *__restrict__ out,
+                               uint32_t *__restrict__ n_out) {
+  const uint32_t k = *kept;
+  uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += stride) out[i] = in[perm[i]];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = k;
+}
+
+// The scratch's device address, looked up once per device with that device
+// current (host code cannot use the symbol itself as a device pointer).
+int noalloc_scratch(int device, uint32_t **out) {
+  static uint32_t *addr[64] = {nullptr};
+  static std::mutex mu;
+  if (device < 0 || device >= 64) return fail(HZ_E_INVALID, "device %d out of range", device);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void *p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess) return fail(HZ_E_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(err));
+    addr[device] = static_cast<uint32_t *>(p);
+  }
+  *out = addr[device];
+  return HZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hz_dedup_and_order_device_noalloc(const hz_segment_pair *d_in, uint32_t n, hz_segment_pair *d_out,
+                                      uint32_t *d_n_out, void *stream) {
+  if (n > kNoAllocMax)
+    return fail(HZ_E_INVALID, "%u HSPs exceed the %u that this entry point's fixed scratch holds", n, kNoAllocMax);
+  if (!d_n_out || (n && (!d_in || !d_out))) return fail(HZ_E_INVALID, "null device pointer");
+  if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out) |
+       reinterpret_cast<uintptr_t>(d_n_out)) & 3)
+    return fail(HZ_E_INVALID, "device buffers must be 4-byte aligned");
+  int device = 0;
+  CK(cudaGetDevice(&device));
+  uint32_t *base = nullptr;
+  TRY(noalloc_scratch(device, &base));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint32_t *perm_a = base, *perm_b = perm_a + kNoAllocMax, *keys_a = perm_b + kNoAllocMax,
+           *keys_b = keys_a + kNoAllocMax, *dropped = keys_b + kNoAllocMax, *hist = dropped + kNoAllocMax,
+           *partials = hist + kNoAllocHist, *total = partials + kNoAllocPartials, *kept = total + 1;
+  // the kept count accumulates and must start at zero; everything else is
+  // fully rewritten before it is read
+  CK(cudaMemsetAsync(kept, 0, 4, s));
+  const PlainHsp *in = reinterpret_cast<const PlainHsp *>(d_in);
+  const unsigned g = grid_for(n, 256, 1024);
+  iota_kernel<<<g, 256, 0, s>>>(perm_a, n);
+  const uint64_t tiles = (n + kRadixTile - 1) / kRadixTile;
+  auto sort_by = [&](const int *fields, int nf) {
+    for (int fi = 0; fi < nf; fi++) {
+      const int f = fields[fi];
+      na_gather_kernel<<<g, 256, 0, s>>>(in, perm_a, dropped, n, f, keys_a);
+      const int passes = f == kDroppedField ? 1 : 4;
+      for (int p = 0; p < passes && n; p++) {
+        radix_hist_kernel<<<(unsigned)tiles, kRadixThreads, 0, s>>>(keys_a, n, 8 * p, hist, tiles);
+        exclusive_scan<uint32_t>(hist, hist, tiles * kRadixBins, partials, total, s);
+        radix_scatter_kernel<<<(unsigned)tiles, kRadixThreads, 0, s>>>(keys_a, perm_a, n, 8 * p, hist, tiles,
+                                                                      keys_b, perm_b);
+        std::swap(keys_a, keys_b);
+        std::swap(perm_a, perm_b);
+      }
+    }
+  };
+  static const int by_diagonal_key[4] = {kScoreDesc, kLen, kRefStart, kDiag};
+  // dropped records last, the kept ones in LASTZ order first
+  static const int by_lastz_key[5] = {kScoreDesc, kLen, kRefStart, kQueryStart, kDroppedField};
+  if (n) {
+    sort_by(by_diagonal_key, 4);
+    na_flag_kernel<<<g, 256, 0, s>>>(in, perm_a, n, dropped, kept);
+    sort_by(by_lastz_key, 5);
+  }
+  na_copy_kernel<<<g, 256, 0, s>>>(in, perm_a, kept, reinterpret_cast<PlainHsp *>(d_out), d_n_out);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return fail(HZ_E_CUDA, "dedup launch: %s", cudaGetErrorString(err));
   return HZ_OK;
 }
 

@@ -165,6 +165,28 @@ int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *s
  * the kept count in *n_out. */
 int hz_dedup_and_order(hz_segment_pair *h, uint64_t n, uint64_t *n_out);
 
+/* No counterpart in the reference.  dedup_and_order of one set of HSPs that
+ * already sits in device memory, for callers that cannot allocate device
+ * memory themselves or let a library do it -- e.g. a host whose own
+ * allocator owns the whole device, or a serving loop that admits work
+ * against a fixed memory budget.  It allocates nothing: its working memory is
+ * a fixed array of about 6 MB compiled into this library, which every GPU
+ * that loads the library holds until the process exits.
+ *   d_in:    n records on the current device (4-byte aligned), read only;
+ *            n <= HZ_NOALLOC_MAX_HSPS, larger n is refused with HZ_E_INVALID.
+ *   d_out:   room for n records; receives the kept records in LASTZ order.
+ *   d_n_out: one device uint32, receives the kept count.
+ *   stream:  a cudaStream_t (NULL for the default stream).
+ * The work is queued on `stream` and the call returns at once; results are
+ * valid once the stream reaches that point.  The first call on a device
+ * looks up the scratch array's device address, so make it before any stream
+ * capture.  All calls share the one scratch array: calls whose work overlaps
+ * on the GPU (other streams, other host threads) race and corrupt each
+ * other's results, so keep them ordered on one stream. */
+#define HZ_NOALLOC_MAX_HSPS (1u << 18)
+int hz_dedup_and_order_device_noalloc(const hz_segment_pair *d_in, uint32_t n, hz_segment_pair *d_out,
+                                      uint32_t *d_n_out, void *stream);
+
 /* Per-kernel device time (CUDA events on the engine's stream) since the last
  * reset; enable with hz_engine_set_profiling.  Entry i: name, total ms,
  * launches.  Returns HZ_E_INVALID past the last entry. */
