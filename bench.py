@@ -9,6 +9,11 @@ one transition, HOXD70, X-drop 910, HSP threshold 3000, both strands.
 --config 3: a resident 200 Mbp target against 512 query chunks with
 log-uniform lengths in 10 kbp-2 Mbp carrying planted homology at 5-35%.
 
+--config 4: repeat-dense 1 Gbp target (10 bins) vs 1 Gbp query with a
+per-seed occurrence cap of 1000.  --config 5: the serving loop over a
+resident 3 Gbp target under a Poisson request stream (p50/p99 latency and
+throughput; see run_serving).
+
 A step is one full pass of every bin x every query x interval x strand x
 WGA chunk.  Two forms are timed: the plain per-chunk form (one launch chain
 and one read-back per seed_and_filter call, as the reference runs) and the
@@ -16,7 +21,7 @@ batched form (all calls of a bin in shared waves: one lookup, one persistent
 gate launch over a device work queue, one read-back per wave).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config 2|3] [--form both|batched|plain] [--scale S]
+                  [--config 2|3|4|5] [--form both|batched|plain] [--scale S]
 
 One JSON line on rank 0.  `value` is seed hits/s over all ranks for the
 batched form with targets and queries resident in HBM; `e2e` is the same
@@ -57,20 +62,47 @@ def workload(config: int, scale: float):
     if config == 3:
         target, chunks = synth.config3(seed=3, scale=scale)
         return [target], chunks
+    if config == 4:
+        t, q = synth.config4(seed=4, scale=scale)
+        step = -(-t.size // 10)
+        return [t[i:i + step] for i in range(0, t.size, step)], [q]
     bins, query = synth.config2(seed=2, scale=scale)
     return bins, [query]
 
 
+def occ_cap(config: int) -> int:
+    return 1000 if config == 4 else 0
+
+
+WORKLOADS = {
+    2: "config2: 100 Mbp target as 10 bins x 10 Mbp vs 100 Mbp query",
+    3: "config3: 200 Mbp resident target vs 512 query chunks (log-uniform 10 kbp-2 Mbp)",
+    4: "config4: repeat-dense 1 Gbp target as 10 bins vs 1 Gbp query (45% from 500 repeat families, "
+       "3% tandem), occurrence cap 1000",
+    5: "config5: serving, resident 3 Gbp target, Poisson arrivals, lognormal(200 kbp, sigma 1) requests "
+       "capped at 5 Mbp, 40 GB admission budget",
+}
+
+
 def config_block(args, n_gpus, bins, queries):
-    name = ("config2: 100 Mbp target as 10 bins x 10 Mbp vs 100 Mbp query" if args.config == 2 else
-            "config3: 200 Mbp resident target vs 512 query chunks (log-uniform 10 kbp-2 Mbp)")
+    name = WORKLOADS[args.config]
     if args.scale != 1.0:
         name += f", scaled x{args.scale}"
     return {"workload": name + ", both strands", "target_bp": int(sum(b.size for b in bins)),
             "query_bp": int(sum(q.size for q in queries)), "bins": len(bins), "queries": len(queries),
             "seed": "12of19", "transitions": True, "xdrop": 910, "hspthresh": 3000, "max_hits": 16711680,
-            "wga_chunk": 250000, "interval": 10000000, "parallelism": f"replicas x{n_gpus}",
-            "l2": "inputs larger than L2 (126 MB)"}
+            "occ_cap": occ_cap(args.config), "wga_chunk": 250000, "interval": 10000000,
+            "parallelism": f"replicas x{n_gpus}", "l2": "inputs larger than L2 (126 MB)"}
+
+
+def over_ranks(vals, op: str, device) -> list:
+    """Element-wise max or sum of `vals` over all ranks (every rank calls it
+    at the same point, with the same length)."""
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    red = {"max": torch.distributed.ReduceOp.MAX, "sum": torch.distributed.ReduceOp.SUM}[op]
+    torch.distributed.all_reduce(t, op=red)
+    return [float(x) for x in t.tolist()]
 
 
 # ---------------------------------------------------------------------------
@@ -130,7 +162,7 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-def cpu_sample(bins, queries, threads: int, budget_batches: int):
+def cpu_sample(bins, queries, threads: int, budget_batches: int, cap: int = 0):
     """The oracle (C restatement of the reference's path) on bin 0 x the
     first `budget_batches` calls of query 0's pass, all host threads;
     returns (hits/s, stats, seconds)."""
@@ -143,7 +175,7 @@ def cpu_sample(bins, queries, threads: int, budget_batches: int):
     qr = oracle.encode(S.reverse_complement_bytes(q).tobytes())
     sh = oracle.shape("12of19")
     idx, pos = oracle.seed_table(ref, sh)
-    p = oracle.params(build_sub_mat("", 910), threads=threads)
+    p = oracle.params(build_sub_mat("", 910), threads=threads, occ_cap=cap)
     t0 = time.perf_counter()
     _, st = oracle.seed_and_filter_all(p, sh, ref, idx, pos, qf, qr, max_batches=budget_batches)
     dt = time.perf_counter() - t0
@@ -166,7 +198,7 @@ def run_reference(args, rank):
     vals = []
     st = dt = None
     for i in range(args.warmup + args.steps):
-        v, st, dt = cpu_sample(bins, queries, threads, args.cpu_batches)
+        v, st, dt = cpu_sample(bins, queries, threads, args.cpu_batches, occ_cap(args.config))
         if i >= args.warmup:
             vals.append((v, dt))
     v = statistics.median([x[0] for x in vals])
@@ -196,7 +228,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream(dev)
     bins, queries = workload(args.config, args.scale)
-    cfg = EngineConfig()
+    cfg = EngineConfig(occ_cap=occ_cap(args.config))
 
     def barrier():
         if world > 1:
@@ -204,11 +236,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return x if world == 1 else over_ranks([x], "max", dev)[0]
 
     # ---- device-resident: one engine per bin, target and queries resident ----
     engines = []
@@ -361,7 +389,7 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, st, dt = cpu_sample(bins, queries, threads, args.cpu_batches)
+        v, st, dt = cpu_sample(bins, queries, threads, args.cpu_batches, occ_cap(args.config))
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": cpu_sample_text(args, st, dt)}
 
     for e in engines:
@@ -387,24 +415,171 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+def percentile(xs, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def run_serving(args, rank, world, local_rank):
+    """Config 5: the serving loop under an open-loop Poisson request stream.
+
+    A step is one window of --requests query chunks whose arrival times are
+    drawn from a Poisson process of rate --rate; a submit thread issues each
+    request at its arrival time while the main thread collects results.
+    Latency is submit -> finished, as the library records it; throughput is
+    the seed hits of the window over its makespan (first arrival -> last
+    completion), so queueing is inside both.  Serving is host-observed end to
+    end by construction: each request's bases go host -> device and its
+    records device -> host inside the window."""
+    import queue
+    import threading
+
+    import numpy as np
+    import torch
+    from hspz_b200 import Engine, EngineConfig, synth
+    from hspz_b200.build import build
+
+    if rank == 0:
+        build()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    t_gen = time.perf_counter()
+    target = synth.config5_target(seed=5, scale=args.scale)
+    rng = np.random.default_rng(50 + rank)
+    t_gen = time.perf_counter() - t_gen
+    e = Engine(EngineConfig(), device=local_rank)
+    t_load = time.perf_counter()
+    e.load_target(target)
+    t_load = time.perf_counter() - t_load
+    budget = int(args.budget_gb * (1 << 30))
+    e.serve_start(budget_bytes=budget, workers=args.workers, max_batch_queries=args.max_batch)
+
+    def window(rate, n_req):
+        lens = synth.request_lengths(rng, n_req)
+        reqs = [synth.serving_request(rng, target, int(L)) for L in lens]
+        arrive = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        arrive -= arrive[0]
+        st0, _, _ = e.serve_stats()
+        tq = queue.Queue()
+        t0 = time.perf_counter()
+
+        def submitter():
+            for a, r in zip(arrive.tolist(), reqs):
+                d = t0 + a - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ts = time.perf_counter() - t0
+                tq.put((e.serve_submit(r), ts))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        out = []
+        for _ in range(n_req):
+            ticket, ts = tq.get()
+            recs, tm = e.serve_poll(ticket)
+            out.append(dict(tm, submit_s=ts, records=int(recs.size), bytes_out=int(recs.nbytes)))
+        th.join()
+        st1, _, _ = e.serve_stats()
+        makespan = max(o["submit_s"] + o["total_ms"] / 1000 for o in out)
+        d = {k: st1[k] - st0[k] for k in st1}
+        return {"makespan_s": makespan, "stats": d, "reqs": out, "bases": int(sum(lens)), "rate": rate}
+
+    for _ in range(args.warmup):
+        window(args.rate, 4)
+    l0 = e.launches
+    with Clocks(local_rank) as clk:
+        runs = [window(args.rate, args.requests) for _ in range(args.steps)]
+    launches = e.launches - l0
+    sweep = []
+    for r in [float(x) for x in args.sweep.split(",") if x.strip()]:
+        w = window(r, args.sweep_requests)
+        lat = [o["total_ms"] for o in w["reqs"]]
+        sweep.append({"rate_req_per_s": r, "requests": args.sweep_requests,
+                      "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
+                      "hits_per_s": w["stats"]["hits"] / w["makespan_s"],
+                      "served_req_per_s": args.sweep_requests / w["makespan_s"],
+                      "mean_batch": float(np.mean([o["batch_queries"] for o in w["reqs"]]))})
+    e.serve_stop()
+    e.close()
+
+    span = sum(r["makespan_s"] for r in runs)
+    hits = sum(r["stats"]["hits"] for r in runs)
+    cells = sum(r["stats"]["cells"] for r in runs)
+    n_req = sum(len(r["reqs"]) for r in runs)
+    if world > 1:
+        span_all = over_ranks([span], "max", dev)[0]
+        hits_all, cells_all = over_ranks([hits, cells], "sum", dev)
+    else:
+        span_all, hits_all, cells_all = span, hits, cells
+    if rank != 0:
+        return
+    lat = [o["total_ms"] for r in runs for o in r["reqs"]]
+    qd = [o["queued_ms"] for r in runs for o in r["reqs"]]
+    sv = [o["service_ms"] for r in runs for o in r["reqs"]]
+    mean_hits = hits / max(n_req, 1)
+    h2d = sum(r["bases"] for r in runs) // max(args.steps, 1)
+    d2h = sum(o["bytes_out"] for r in runs for o in r["reqs"]) // max(args.steps, 1)
+    value = hits_all / span_all
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": span_all / args.steps * 1000, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": WORKLOADS[5] + (f", target scaled x{args.scale}" if args.scale != 1.0 else ""),
+                       "target_bp": int(target.size), "rate_req_per_s": args.rate,
+                       "requests_per_step": args.requests, "workers": args.workers,
+                       "max_batch_queries": args.max_batch, "budget_bytes": budget,
+                       "seed": "12of19", "transitions": True, "xdrop": 910, "hspthresh": 3000,
+                       "max_hits": 16711680, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (126 MB)", "timing": "host clock, submit -> finished"},
+            "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99), "mean": float(np.mean(lat)),
+                           "queued_p50": percentile(qd, 50), "queued_p99": percentile(qd, 99),
+                           "service_p50": percentile(sv, 50), "service_p99": percentile(sv, 99)},
+            "served_req_per_s": n_req / span, "offered_req_per_s": args.rate,
+            "mean_hits_per_request": mean_hits, "offered_hits_per_s": mean_hits * args.rate,
+            "extended_bp_per_s": cells_all / span_all,
+            "mean_batch_queries": float(np.mean([o["batch_queries"] for r in runs for o in r["reqs"]])),
+            "rate_sweep": sweep, "gpu_launches": launches, "clocks": clk.summary(),
+            "setup_s": {"target_generation": t_gen, "load_target": t_load},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "note": "serving is measured end to end; value and e2e are the same measurement"},
+            "cpu_baseline": None,
+            "cpu_note": "the CPU path is timed on configs 2-4; a 3 Gbp host seed table is out of a bench budget"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[2, 3])
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5])
     ap.add_argument("--form", default="both", choices=["both", "batched", "plain"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-batches", type=int, default=80)
     ap.add_argument("--tuning", default="", help='JSON of engine launch knobs, e.g. {"gate_tile": 4096}')
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--rate", type=float, default=50.0, help="config 5: Poisson arrival rate, requests/s")
+    ap.add_argument("--requests", type=int, default=32, help="config 5: requests per timed window")
+    ap.add_argument("--sweep", default="2,5", help="config 5: extra arrival rates, one window each")
+    ap.add_argument("--sweep-requests", type=int, default=12)
+    ap.add_argument("--workers", type=int, default=2, help="config 5: serving worker threads")
+    ap.add_argument("--max-batch", type=int, default=16, help="config 5: queries per batch at most")
+    ap.add_argument("--budget-gb", type=float, default=40.0, help="config 5: admission budget")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        if args.config == 5:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT,
+                                  "unavailable": "the reference has no serving loop; its CPU path is timed on "
+                                                 "configs 2-4"}), flush=True)
+            return
         run_reference(args, rank)
         return
     if world > 1:
@@ -414,7 +589,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                              device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.config == 5:
+            run_serving(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch

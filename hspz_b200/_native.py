@@ -55,6 +55,18 @@ class QueryC(C.Structure):
     _fields_ = [("ascii", C.c_void_p), ("len", C.c_uint64)]
 
 
+class ServeConfigC(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("workers", C.c_uint32), ("max_batch_queries", C.c_uint32)]
+
+
+class ServeTimesC(C.Structure):
+    _fields_ = [("queued_ms", C.c_double), ("service_ms", C.c_double), ("total_ms", C.c_double),
+                ("batch_queries", C.c_uint32), ("worker", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 # (name, restype, argtypes) of every exported entry point.
@@ -87,6 +99,12 @@ SIGNATURES = {
     "hz_engine_launches": (U64, [P]),
     "hz_engine_set_stream": (C.c_int, [P, P]),
     "hz_engine_set_tuning": (C.c_int, [P, C.c_char_p, C.c_int64]),
+    "hz_serve_start": (C.c_int, [P, C.POINTER(ServeConfigC)]),
+    "hz_serve_submit": (C.c_int, [P, P, U64, PU64]),
+    "hz_serve_poll": (C.c_int, [P, U64, C.c_int, C.POINTER(P), PU64, C.POINTER(ServeTimesC)]),
+    "hz_serve_stats": (C.c_int, [P, C.POINTER(StatsC), PU64, PU64]),
+    "hz_serve_cancel": (C.c_int, [P, U64]),
+    "hz_serve_stop": (C.c_int, [P]),
 }
 
 

@@ -14,6 +14,12 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <thread>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -237,6 +243,9 @@ struct WaveRecord {
   hz_segment_pair h;
 };
 
+struct Server;
+uint64_t server_launches(Server *s);  // kernel launches of a serving loop's workers
+
 struct hz_engine {
   int device = 0;
   int sm_count = 148;
@@ -253,6 +262,8 @@ struct hz_engine {
   DBuf<uint32_t> pos_table;
   uint64_t n_pos = 0;
   bool has_target = false;
+  bool owns_target = true;         // false for serving workers that share the owner's tables
+  struct Server *server = nullptr;  // the serving loop, while one runs
   // query store
   SeqBuf qstore;
   DBuf<uint8_t> qascii;
@@ -350,10 +361,14 @@ template <int TILE> size_t gate_smem() { return sizeof(GateSmem<TILE>); }
 
 template <int TILE> int launch_gate(hz_engine *e, const GateArgs &ga) {
   static bool configured[64] = {false};
+  static std::mutex mu;  // serving workers launch from several host threads
   size_t smem = gate_smem<TILE>();
-  if (!configured[e->device & 63]) {
-    CK(cudaFuncSetAttribute(gate_kernel<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured[e->device & 63] = true;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!configured[e->device & 63]) {
+      CK(cudaFuncSetAttribute(gate_kernel<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured[e->device & 63] = true;
+    }
   }
   int per_sm = e->gate_blocks_per_sm;
   if (per_sm <= 0) {
@@ -680,6 +695,27 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
   return HZ_OK;
 }
 
+// The batched form over every staged query: the calls, query-major, cut into
+// waves of at most wave_positions seed positions at call boundaries.
+// *recs[k].call indexes *calls.
+int run_all_staged(hz_engine *e, std::vector<HostCall> *calls, std::vector<WaveRecord> *recs, hz_stats *st) {
+  for (uint32_t q = 0; q < e->queries.size(); q++) query_calls(e, q, calls);
+  size_t i = 0;
+  while (i < calls->size()) {
+    size_t j = i;
+    uint64_t npos = 0;
+    while (j < calls->size() && (j == i || npos + ((*calls)[j].end - (*calls)[j].start) <= e->wave_positions)) {
+      npos += (*calls)[j].end - (*calls)[j].start;
+      j++;
+    }
+    size_t before = recs->size();
+    TRY(run_wave(e, calls->data() + i, j - i, nullptr, e->cfg.transitions, recs, st, e->device_dedup));
+    for (size_t k = before; k < recs->size(); k++) (*recs)[k].call += (uint32_t)i;
+    i = j;
+  }
+  return HZ_OK;
+}
+
 int check_range(hz_engine *e, uint32_t start, uint32_t end) {
   if (end < start) return fail(HZ_E_INVALID, "seed range [%u, %u) is reversed", start, end);
   uint32_t qlen = e->queries.empty() ? 0 : e->queries[e->cur_query].len;
@@ -784,9 +820,12 @@ void hz_engine_destroy(hz_engine *e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->st) cudaStreamSynchronize(e->st);
-  e->ref.buf.release();
-  e->index_table.release();
-  e->pos_table.release();
+  if (e->server) hz_serve_stop(e);
+  if (e->owns_target) {
+    e->ref.buf.release();
+    e->index_table.release();
+    e->pos_table.release();
+  }
   e->qstore.buf.release();
   e->qascii.release();
   for (auto &s : e->slot) s.seeds.release();
@@ -826,6 +865,7 @@ void hz_engine_destroy(hz_engine *e) {
 int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t index_len, const uint32_t *pos_table,
                           uint64_t pos_len, const uint8_t *ref_seq, uint64_t ref_len) {
   if (!e || !index_table || (ref_len && !ref_seq) || (pos_len && !pos_table)) return fail(HZ_E_INVALID, "null argument");
+  if (e->server) return fail(HZ_E_STATE, "the serving loop is running on this target");
   if (index_len != (1ull << (2 * e->shape.kmer_size)))
     return fail(HZ_E_INVALID, "index_table has %llu entries, the seed needs 4^%u", (unsigned long long)index_len,
                 e->shape.kmer_size);
@@ -862,6 +902,7 @@ int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t in
 
 int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) {
   if (!e || (!ref_ascii && len)) return fail(HZ_E_INVALID, "null argument");
+  if (e->server) return fail(HZ_E_STATE, "the serving loop is running on this target");
   if (len > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "reference block exceeds u32 coordinates");
   TRY(set_device(e));
   cudaStream_t st = e->st;
@@ -1183,21 +1224,8 @@ int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *s
   hz_stats local;
   memset(&local, 0, sizeof local);
   std::vector<HostCall> calls;
-  for (uint32_t q = 0; q < e->queries.size(); q++) query_calls(e, q, &calls);
   std::vector<WaveRecord> recs;
-  size_t i = 0;
-  while (i < calls.size()) {
-    size_t j = i;
-    uint64_t npos = 0;
-    while (j < calls.size() && (j == i || npos + (calls[j].end - calls[j].start) <= e->wave_positions)) {
-      npos += calls[j].end - calls[j].start;
-      j++;
-    }
-    size_t before = recs.size();
-    TRY(run_wave(e, calls.data() + i, j - i, nullptr, e->cfg.transitions, &recs, &local, e->device_dedup));
-    for (size_t k = before; k < recs.size(); k++) recs[k].call += (uint32_t)i;
-    i = j;
-  }
+  TRY(run_all_staged(e, &calls, &recs, &local));
   if (!recs.empty()) {
     *out = (hz_batch_record *)malloc(recs.size() * sizeof(hz_batch_record));
     if (!*out) return fail(HZ_E_OOM, "host allocation");
@@ -1400,7 +1428,10 @@ int hz_engine_profile_reset(hz_engine *e) {
   return HZ_OK;
 }
 
-uint64_t hz_engine_launches(hz_engine *e) { return e ? e->launches : 0; }
+uint64_t hz_engine_launches(hz_engine *e) {
+  if (!e) return 0;
+  return e->launches + (e->server ? server_launches(e->server) : 0);
+}
 
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   if (!e || !key) return fail(HZ_E_INVALID, "null argument");
@@ -1431,6 +1462,338 @@ int hz_engine_set_stream(hz_engine *e, void *stream) {
   TRY(set_device(e));
   TRY(e->sync());
   e->st = stream ? (cudaStream_t)stream : e->own_st;
+  return HZ_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving loop.  The engine's target stays resident; worker threads, each
+// with its own workspace (query store, wave buffers, stream) over the shared
+// target tables, keep taking the queued requests that fit the memory budget
+// and run them as one batched pass.  A request that arrives while others are
+// on the GPU joins the next batch a worker forms, so requests are admitted as
+// workers and memory free up, and the batches of different workers overlap on
+// the device.  A request's records equal what hz_run_pass returns for its
+// query alone (tests/test_gpu_serving.py).
+
+enum ServeState { kPending = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
+
+struct ServeRequest {
+  uint64_t ticket = 0;
+  std::vector<uint8_t> ascii;
+  uint64_t est_bytes = 0;
+  int state = kPending;
+  int err = HZ_OK;
+  std::string msg;
+  std::vector<hz_pass_record> recs;
+  uint32_t batch_queries = 0, worker = 0;
+  std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
+};
+
+struct Server {
+  hz_engine *owner = nullptr;
+  std::vector<hz_engine *> workers;
+  std::vector<std::thread> threads;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<uint64_t> pending;
+  std::unordered_map<uint64_t, std::shared_ptr<ServeRequest>> reqs;
+  uint64_t next_ticket = 1;
+  uint64_t budget = 0, in_flight = 0;
+  uint32_t max_batch = 64;
+  bool stopping = false;
+  hz_stats totals{};
+  uint64_t running = 0;
+  uint64_t launches = 0;  // kernel launches of the workers
+};
+
+uint64_t server_launches(Server *s) {
+  std::lock_guard<std::mutex> lock(s->mu);
+  return s->launches;
+}
+
+namespace {
+
+// Device working memory a request needs while it runs: both strands of the
+// query store, per-position counts and compaction, and a margin for the
+// candidate, HSP and dedup buffers.
+uint64_t serve_estimate(uint64_t len) { return 2 * len * (1 + 4 + 12) + (1ull << 20); }
+
+// A workspace that shares `e`'s resident target tables without owning them.
+int clone_shared(hz_engine *e, hz_engine **out) {
+  hz_engine *w = new hz_engine();
+  w->device = e->device;
+  w->sm_count = e->sm_count;
+  w->cfg = e->cfg;
+  w->shape = e->shape;
+  w->max_hits = e->max_hits;
+  w->ref.buf.p = e->ref.buf.p;
+  w->ref.buf.cap = e->ref.buf.cap;
+  w->ref.len = e->ref.len;
+  w->rlen = e->rlen;
+  w->index_table.p = e->index_table.p;
+  w->index_table.cap = e->index_table.cap;
+  w->index_len = e->index_len;
+  w->pos_table.p = e->pos_table.p;
+  w->pos_table.cap = e->pos_table.cap;
+  w->n_pos = e->n_pos;
+  w->has_target = true;
+  w->owns_target = false;
+  w->gate_tile = e->gate_tile;
+  w->gate_cap = e->gate_cap;
+  w->gate_blocks_per_sm = e->gate_blocks_per_sm;
+  w->wave_positions = e->wave_positions;
+  w->device_dedup = e->device_dedup;
+  cudaError_t err = cudaStreamCreateWithFlags(&w->own_st, cudaStreamNonBlocking);
+  if (err != cudaSuccess) {
+    w->owns_target = false;
+    delete w;
+    return fail(HZ_E_CUDA, "worker stream: %s", cudaGetErrorString(err));
+  }
+  w->st = w->own_st;
+  int rc = w->qstore.ensure(0, w->st);
+  if (rc != HZ_OK) {
+    hz_engine_destroy(w);
+    return rc;
+  }
+  *out = w;
+  return HZ_OK;
+}
+
+// The request behind a queued ticket, or null once it was cancelled (and
+// perhaps already polled, which drops it from the ticket map).
+std::shared_ptr<ServeRequest> queued_request(Server *s, uint64_t ticket) {
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end() || it->second->state != kPending) return nullptr;
+  return it->second;
+}
+
+void serve_worker(Server *s, uint32_t index, hz_engine *w) {
+  cudaSetDevice(w->device);
+  while (true) {
+    std::vector<std::shared_ptr<ServeRequest>> batch;
+    {
+      std::unique_lock<std::mutex> lock(s->mu);
+      while (true) {
+        while (!s->pending.empty() && !queued_request(s, s->pending.front())) s->pending.pop_front();
+        if (s->stopping && s->pending.empty()) return;
+        // admit queued requests, in arrival order, while they fit the budget
+        while (!s->pending.empty() && batch.size() < s->max_batch) {
+          auto r = queued_request(s, s->pending.front());
+          if (!r) {
+            s->pending.pop_front();
+            continue;
+          }
+          if (s->in_flight + r->est_bytes > s->budget) break;
+          s->pending.pop_front();
+          r->state = kRunning;
+          r->t_admit = std::chrono::steady_clock::now();
+          s->in_flight += r->est_bytes;
+          s->running += 1;
+          batch.push_back(r);
+        }
+        if (!batch.empty()) break;
+        s->cv_work.wait(lock);
+      }
+    }
+    // one batched pass over the admitted queries
+    std::vector<const uint8_t *> ptrs;
+    std::vector<uint64_t> lens;
+    for (auto &r : batch) {
+      ptrs.push_back(r->ascii.data());
+      lens.push_back(r->ascii.size());
+    }
+    std::vector<HostCall> calls;
+    std::vector<WaveRecord> recs;
+    hz_stats st{};
+    uint64_t l0 = w->launches;
+    int rc = stage_ascii(w, ptrs.data(), lens.data(), (uint32_t)batch.size());
+    if (rc == HZ_OK) rc = run_all_staged(w, &calls, &recs, &st);
+    std::string msg = rc == HZ_OK ? std::string() : g_err;
+    {
+      std::lock_guard<std::mutex> lock(s->mu);
+      auto now = std::chrono::steady_clock::now();
+      if (rc == HZ_OK)
+        for (auto &wr : recs) {
+          const HostCall &c = calls[wr.call];
+          batch[c.query]->recs.push_back(hz_pass_record{c.interval, c.strand, wr.h});
+        }
+      for (auto &r : batch) {
+        r->state = rc == HZ_OK ? kDone : kFailed;
+        r->err = rc;
+        r->msg = msg;
+        r->batch_queries = (uint32_t)batch.size();
+        r->worker = index;
+        r->t_done = now;
+        r->ascii.clear();
+        r->ascii.shrink_to_fit();
+        s->in_flight -= r->est_bytes;
+        s->running -= 1;
+      }
+      s->launches += w->launches - l0;
+      if (rc == HZ_OK) {
+        s->totals.seeds += st.seeds;
+        s->totals.hits += st.hits;
+        s->totals.raw_hsps += st.raw_hsps;
+        s->totals.hsps += st.hsps;
+        s->totals.cells += st.cells;
+        s->totals.calls += st.calls;
+      }
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hz_serve_start(hz_engine *e, const hz_serve_config *cfg) {
+  if (!e || !cfg) return fail(HZ_E_INVALID, "null argument");
+  if (e->server) return fail(HZ_E_STATE, "the serving loop is already running");
+  if (!e->has_target) return fail(HZ_E_STATE, "no target loaded");
+  if (cfg->workers < 1 || cfg->workers > 8) return fail(HZ_E_INVALID, "workers must be 1..8");
+  if (cfg->budget_bytes == 0) return fail(HZ_E_INVALID, "budget_bytes must be > 0");
+  TRY(set_device(e));
+  TRY(e->sync());
+  Server *s = new Server();
+  s->owner = e;
+  s->budget = cfg->budget_bytes;
+  s->max_batch = cfg->max_batch_queries ? cfg->max_batch_queries : 64;
+  for (uint32_t i = 0; i < cfg->workers; i++) {
+    hz_engine *w = nullptr;
+    int rc = clone_shared(e, &w);
+    if (rc != HZ_OK) {
+      for (auto *x : s->workers) hz_engine_destroy(x);
+      delete s;
+      return rc;
+    }
+    s->workers.push_back(w);
+  }
+  e->server = s;
+  for (uint32_t i = 0; i < (uint32_t)s->workers.size(); i++) s->threads.emplace_back(serve_worker, s, i, s->workers[i]);
+  return HZ_OK;
+}
+
+int hz_serve_submit(hz_engine *e, const uint8_t *ascii, uint64_t len, uint64_t *ticket) {
+  if (!e || !ticket || (len && !ascii)) return fail(HZ_E_INVALID, "null argument");
+  Server *s = e->server;
+  if (!s) return fail(HZ_E_STATE, "the serving loop is not running");
+  if (len > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "query block exceeds u32 coordinates");
+  auto r = std::make_shared<ServeRequest>();
+  r->est_bytes = serve_estimate(len);
+  if (r->est_bytes > s->budget)
+    return fail(HZ_E_BUDGET, "a %llu-base query needs ~%llu bytes of working memory, above the %llu-byte budget",
+                (unsigned long long)len, (unsigned long long)r->est_bytes, (unsigned long long)s->budget);
+  r->ascii.assign(ascii, ascii + len);
+  r->t_submit = std::chrono::steady_clock::now();
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->stopping) return fail(HZ_E_STATE, "the serving loop is stopping");
+    r->ticket = s->next_ticket++;
+    s->reqs[r->ticket] = r;
+    s->pending.push_back(r->ticket);
+  }
+  s->cv_work.notify_one();
+  *ticket = r->ticket;
+  return HZ_OK;
+}
+
+int hz_serve_poll(hz_engine *e, uint64_t ticket, int timeout_ms, hz_pass_record **out, uint64_t *n,
+                  hz_serve_times *times) {
+  if (!e || !out || !n) return fail(HZ_E_INVALID, "null argument");
+  *out = nullptr;
+  *n = 0;
+  Server *s = e->server;
+  if (!s) return fail(HZ_E_STATE, "the serving loop is not running");
+  std::unique_lock<std::mutex> lock(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return fail(HZ_E_INVALID, "unknown ticket %llu", (unsigned long long)ticket);
+  auto r = it->second;
+  auto done = [&] { return r->state == kDone || r->state == kFailed || r->state == kCancelled; };
+  if (!done()) {
+    if (timeout_ms < 0) s->cv_done.wait(lock, done);
+    else if (!s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), done))
+      return fail(HZ_E_TIMEOUT, "ticket %llu still %s", (unsigned long long)ticket,
+                  r->state == kPending ? "queued" : "running");
+  }
+  s->reqs.erase(it);
+  if (times) {
+    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    times->queued_ms = r->state == kCancelled ? 0.0 : ms(r->t_submit, r->t_admit);
+    times->service_ms = r->state == kCancelled ? 0.0 : ms(r->t_admit, r->t_done);
+    times->total_ms = r->state == kCancelled ? 0.0 : ms(r->t_submit, r->t_done);
+    times->batch_queries = r->batch_queries;
+    times->worker = r->worker;
+  }
+  if (r->state == kCancelled) return fail(HZ_E_STATE, "ticket %llu was cancelled", (unsigned long long)ticket);
+  if (r->state == kFailed) return fail(r->err, "%s", r->msg.c_str());
+  if (!r->recs.empty()) {
+    *out = (hz_pass_record *)malloc(r->recs.size() * sizeof(hz_pass_record));
+    if (!*out) return fail(HZ_E_OOM, "host allocation");
+    memcpy(*out, r->recs.data(), r->recs.size() * sizeof(hz_pass_record));
+  }
+  *n = r->recs.size();
+  return HZ_OK;
+}
+
+int hz_serve_stats(hz_engine *e, hz_stats *stats, uint64_t *queued, uint64_t *running) {
+  if (!e) return fail(HZ_E_INVALID, "null engine");
+  Server *s = e->server;
+  if (!s) return fail(HZ_E_STATE, "the serving loop is not running");
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (stats) *stats = s->totals;
+  if (queued) {
+    uint64_t q = 0;
+    for (uint64_t t : s->pending)
+      if (queued_request(s, t)) q++;
+    *queued = q;
+  }
+  if (running) *running = s->running;
+  return HZ_OK;
+}
+
+int hz_serve_cancel(hz_engine *e, uint64_t ticket) {
+  if (!e) return fail(HZ_E_INVALID, "null engine");
+  Server *s = e->server;
+  if (!s) return fail(HZ_E_STATE, "the serving loop is not running");
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return fail(HZ_E_INVALID, "unknown ticket %llu", (unsigned long long)ticket);
+    if (it->second->state != kPending)
+      return fail(HZ_E_STATE, "ticket %llu is already running or finished", (unsigned long long)ticket);
+    it->second->state = kCancelled;
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();
+  return HZ_OK;
+}
+
+int hz_serve_stop(hz_engine *e) {
+  if (!e) return fail(HZ_E_INVALID, "null engine");
+  Server *s = e->server;
+  if (!s) return HZ_OK;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stopping = true;
+  }
+  s->cv_work.notify_all();
+  for (auto &t : s->threads) t.join();
+  for (auto *w : s->workers) hz_engine_destroy(w);
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (auto &kv : s->reqs)
+      if (kv.second->state == kPending) kv.second->state = kCancelled;
+  }
+  s->cv_done.notify_all();
+  e->launches += s->launches;
+  e->server = nullptr;
+  delete s;
   return HZ_OK;
 }
 

@@ -216,6 +216,40 @@ class Engine:
     def launches(self) -> int:
         return int(N.lib().hz_engine_launches(self._h))
 
+    # --- serving loop ---------------------------------------------------------
+    def serve_start(self, budget_bytes: int, workers: int = 2, max_batch_queries: int = 0):
+        """Start worker threads that take submitted query blocks as they
+        arrive, batching those that fit the device memory budget."""
+        cfg = N.ServeConfigC(budget_bytes=int(budget_bytes), workers=int(workers),
+                             max_batch_queries=int(max_batch_queries))
+        N.check(N.lib().hz_serve_start(self._h, C.byref(cfg)))
+
+    def serve_submit(self, query_ascii) -> int:
+        a = np.ascontiguousarray(as_bytes(query_ascii))
+        t = C.c_uint64()
+        N.check(N.lib().hz_serve_submit(self._h, _ptr(a) if a.size else None, a.size, C.byref(t)))
+        return t.value
+
+    def serve_poll(self, ticket: int, timeout_ms: int = -1):
+        """(records like run_pass, timings) for a finished ticket; raises
+        HzError (HZ_E_TIMEOUT while it is still queued or running)."""
+        out, n, tm = C.c_void_p(), C.c_uint64(), N.ServeTimesC()
+        N.check(N.lib().hz_serve_poll(self._h, int(ticket), int(timeout_ms), C.byref(out), C.byref(n),
+                                      C.byref(tm)))
+        return _take(out, n.value, PASS_RECORD), tm.as_dict()
+
+    def serve_stats(self):
+        """(totals over finished batches, requests queued, requests running)."""
+        st, q, r = N.StatsC(), C.c_uint64(), C.c_uint64()
+        N.check(N.lib().hz_serve_stats(self._h, C.byref(st), C.byref(q), C.byref(r)))
+        return st.as_dict(), q.value, r.value
+
+    def serve_cancel(self, ticket: int):
+        N.check(N.lib().hz_serve_cancel(self._h, int(ticket)))
+
+    def serve_stop(self):
+        N.check(N.lib().hz_serve_stop(self._h))
+
 
 def dedup_and_order(h: np.ndarray) -> np.ndarray:
     """dedup_and_order (src/hsp.rs:94-126) through the library's host code."""

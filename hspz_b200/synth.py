@@ -82,6 +82,11 @@ def soft_mask(rng: np.random.Generator, s: np.ndarray, frac: float = 0.10, lo: i
     k = int(n * frac / mean) + 1
     starts = rng.integers(0, n, k)
     lens = rng.integers(lo, hi + 1, k)
+    if n > (1 << 28):  # same result without an n-sized counter array
+        s = s.copy()
+        for a, l in zip(starts.tolist(), lens.tolist()):
+            s[a: a + l] |= 0x20
+        return s
     mask = np.zeros(n + 1, dtype=np.int32)
     np.add.at(mask, starts, 1)
     np.add.at(mask, np.minimum(starts + lens, n), -1)
@@ -165,3 +170,81 @@ def config3(seed: int = 3, scale: float = 1.0, n_chunks: int = 512, homology_fra
         plant(rng, t, q, n_seg, 200, 5000, 0.05, 0.35)
         chunks.append(soft_mask(rng, q))
     return soft_mask(rng, t), chunks
+
+
+def random_genome(rng: np.random.Generator, n: int, piece: int = 1 << 26) -> np.ndarray:
+    """random_bases for genome-sized n, drawn in pieces to bound host memory."""
+    out = np.empty(n, dtype=np.uint8)
+    for a in range(0, n, piece):
+        out[a: a + piece] = random_bases(rng, min(piece, n - a))
+    return out
+
+
+def repeat_families(rng: np.random.Generator, n_fam: int = 500, lo: int = 300, hi: int = 6000):
+    """Consensus sequences of the interspersed repeat families."""
+    return [random_bases(rng, int(L)) for L in rng.integers(lo, hi + 1, n_fam)]
+
+
+def repeat_genome(rng: np.random.Generator, n: int, families, rep_frac: float = 0.45,
+                  tandem_frac: float = 0.03, rate_lo: float = 0.05, rate_hi: float = 0.30) -> np.ndarray:
+    """Background sequence with ~rep_frac of it copies of the families (whole
+    consensus, U[rate_lo, rate_hi] substitutions, half reverse-complemented)
+    laid end to end between random gaps, then ~tandem_frac of it tandem arrays
+    (unit U[2, 50] bp, array U[100, 5000] bp, 0-10% substitutions)."""
+    s = random_genome(rng, n)
+    mean_copy = float(np.mean([f.size for f in families]))
+    mean_gap = mean_copy * (1.0 - rep_frac) / max(rep_frac, 1e-9)
+    pos = int(rng.exponential(mean_gap))
+    while pos < n:
+        f = families[int(rng.integers(len(families)))]
+        seg = mutate(rng, f, float(rng.uniform(rate_lo, rate_hi)))
+        if rng.random() < 0.5:
+            seg = revcomp(seg)
+        seg = seg[: n - pos]
+        s[pos: pos + seg.size] = seg
+        pos += seg.size + int(rng.exponential(mean_gap))
+    placed, want = 0, int(n * tandem_frac)
+    while placed < want:
+        unit = random_bases(rng, int(rng.integers(2, 51)))
+        L = int(rng.integers(100, 5001))
+        arr = mutate(rng, np.resize(unit, L), float(rng.uniform(0.0, 0.10)))
+        a = int(rng.integers(0, max(1, n - L)))
+        arr = arr[: n - a]
+        s[a: a + arr.size] = arr
+        placed += arr.size
+    return s
+
+
+def config4(seed: int = 4, scale: float = 1.0):
+    """Repeat-dense pair: 1 Gbp target and 1 Gbp query, each ~45% copies of
+    500 shared repeat families (consensus 300-6000 bp, 5-30% divergence) and
+    ~3% tandem repeats (unit 2-50 bp), plus planted orthologous segments;
+    the run uses a per-seed occurrence cap of 1000."""
+    rng = np.random.default_rng(seed)
+    n = int(1_000_000_000 * scale)
+    fam = repeat_families(rng)
+    t = repeat_genome(rng, n, fam)
+    q = repeat_genome(rng, n, fam)
+    plant(rng, t, q, max(1, int(20_000 * scale)), 200, 5000, 0.10, 0.30, indel_rate=0.01)
+    return soft_mask(rng, t), soft_mask(rng, q)
+
+
+def config5_target(seed: int = 5, scale: float = 1.0) -> np.ndarray:
+    """Resident serving target: a 3 Gbp synthetic genome (soft-masked ~10%)."""
+    rng = np.random.default_rng(seed)
+    return soft_mask(rng, random_genome(rng, int(3_000_000_000 * scale)))
+
+
+def request_lengths(rng: np.random.Generator, n: int, median: float = 200_000, sigma: float = 1.0,
+                    cap: int = 5_000_000, lo: int = 1000) -> np.ndarray:
+    """Serving request lengths: lognormal(ln median, sigma), capped."""
+    return np.clip(rng.lognormal(np.log(median), sigma, n), lo, cap).astype(np.int64)
+
+
+def serving_request(rng: np.random.Generator, target: np.ndarray, length: int,
+                    homology_frac: float = 0.2) -> np.ndarray:
+    """One query chunk with planted homology to the target over ~homology_frac
+    of its length (segments U[200, 5000] at 5-35% divergence)."""
+    q = random_bases(rng, int(length))
+    plant(rng, target, q, max(1, int(length * homology_frac / 2600)), 200, 5000, 0.05, 0.35)
+    return soft_mask(rng, q)

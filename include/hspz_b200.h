@@ -203,12 +203,61 @@ int hz_engine_profile_reset(hz_engine *e);
  * batched form dedups on the device, 0: on the host as the plain form does). */
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
 
-/* Kernel launches issued by this engine since creation. */
+/* Kernel launches issued by this engine since creation, its serving
+ * workers' included. */
 uint64_t hz_engine_launches(hz_engine *e);
 
 /* Runs the engine's work on a caller-owned cudaStream_t (NULL restores the
  * engine's own stream), so callers can order and time it with their events. */
 int hz_engine_set_stream(hz_engine *e, void *stream);
+
+/* ---- serving loop ------------------------------------------------------
+ * The reference runs one bin of queries at a time (run_bins,
+ * src/run.rs:816-887) and has no request queue; these entry points keep a
+ * target resident and take query blocks as they arrive.  hz_serve_start
+ * starts `workers` host threads, each with its own query store, wave buffers
+ * and stream over the engine's target tables.  A free worker takes the queued
+ * requests in arrival order while their estimated device working memory fits
+ * under `budget_bytes` (at most `max_batch_queries` of them, 0 = 64) and runs
+ * them as one batched pass, so requests that arrive while others run join the
+ * next batch.  A request's records equal what hz_run_pass returns for that
+ * query block alone. */
+typedef struct hz_serve_config {
+  uint64_t budget_bytes;       /* device working memory for requests in flight */
+  uint32_t workers;            /* 1..8 */
+  uint32_t max_batch_queries;  /* 0 = 64 */
+} hz_serve_config;
+
+typedef struct hz_serve_times {
+  double queued_ms;        /* submit -> taken by a worker */
+  double service_ms;       /* taken -> its batch finished */
+  double total_ms;         /* submit -> finished */
+  uint32_t batch_queries;  /* queries in the batch it ran in */
+  uint32_t worker;         /* index of the worker that ran it */
+} hz_serve_times;
+
+/* HZ_E_STATE if a loop already runs or no target is loaded.  While the loop
+ * runs, the engine's own entry points that touch the target are refused. */
+int hz_serve_start(hz_engine *e, const hz_serve_config *cfg);
+/* Copies the query block; HZ_E_BUDGET if its estimated working memory alone
+ * exceeds the budget (it could never be admitted). */
+int hz_serve_submit(hz_engine *e, const uint8_t *ascii, uint64_t len, uint64_t *ticket);
+/* Waits up to timeout_ms (< 0: without limit) for the ticket.  HZ_E_TIMEOUT
+ * if it has not finished (the ticket stays valid); otherwise the ticket is
+ * consumed and either *out holds its records (hz_pass_record, freed with
+ * hz_free) or the call returns the request's own error (HZ_E_STATE for a
+ * cancelled one).  HZ_E_INVALID for an unknown or consumed ticket. */
+int hz_serve_poll(hz_engine *e, uint64_t ticket, int timeout_ms, hz_pass_record **out, uint64_t *n,
+                  hz_serve_times *times);
+/* Totals (seeds, hits, cells, HSPs, calls) over every batch finished since
+ * hz_serve_start, and the requests still queued or running. */
+int hz_serve_stats(hz_engine *e, hz_stats *stats, uint64_t *queued, uint64_t *running);
+/* Cancels a request that no worker has taken yet (HZ_E_STATE otherwise). */
+int hz_serve_cancel(hz_engine *e, uint64_t ticket);
+/* Finishes every queued request, joins the workers and frees their memory.
+ * Tickets not polled before the stop are dropped.  No other serving entry
+ * point may run on the engine while it stops. */
+int hz_serve_stop(hz_engine *e);
 
 #ifdef __cplusplus
 }
