@@ -249,6 +249,15 @@ def run_ours(args, rank, world, local_rank):
         e.stage_queries(queries)
         engines.append(e)
 
+    tuning = None
+    if not args.no_autotune:
+        # launch shapes timed on a sample of this workload (outside the timed
+        # region), then used by every engine of both forms
+        tuning = engines[0].autotune(sample_positions=args.tune_positions)
+        knobs = {k: tuning[k] for k in ("gate_tile", "gate_cap", "graph")}
+        for e in engines:
+            e.set_tuning(**knobs)
+
     def step(form):
         tot = {"hits": 0, "cells": 0, "raw_hsps": 0, "hsps": 0, "seeds": 0, "calls": 0}
         recs = []
@@ -356,6 +365,10 @@ def run_ours(args, rank, world, local_rank):
         pin_b = [torch.from_numpy(b).pin_memory() for b in bins]
         e2 = Engine(cfg, device=local_rank)
         e2.set_stream(stream.cuda_stream)
+        if args.tuning:
+            e2.set_tuning(**json.loads(args.tuning))
+        if tuning:
+            e2.set_tuning(**{k: tuning[k] for k in ("gate_tile", "gate_cap", "graph")})
         L = N.lib()
         qarr = (N.QueryC * len(pin_q))()
         for i, t in enumerate(pin_q):
@@ -411,7 +424,8 @@ def run_ours(args, rank, world, local_rank):
             "forms": summ,
             "batched_over_plain": (summ["batched"]["hits_per_s"] / summ["plain"]["hits_per_s"]
                                    if len(summ) == 2 else None),
-            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"], "e2e": e2e, "cpu_baseline": cpu}
+            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"], "e2e": e2e, "cpu_baseline": cpu,
+            "autotune": tuning}
     print(json.dumps(line), flush=True)
 
 
@@ -455,6 +469,12 @@ def run_serving(args, rank, world, local_rank):
     e.load_target(target)
     t_load = time.perf_counter() - t_load
     budget = int(args.budget_gb * (1 << 30))
+    tuning = None
+    if not args.no_autotune:
+        # launch shapes tuned on a few requests of this stream before it starts;
+        # the workers inherit them
+        e.stage_queries([synth.serving_request(rng, target, int(L)) for L in synth.request_lengths(rng, 4)])
+        tuning = e.autotune(sample_positions=1 << 22)
     e.serve_start(budget_bytes=budget, workers=args.workers, max_batch_queries=args.max_batch)
 
     def window(rate, n_req):
@@ -540,7 +560,7 @@ def run_serving(args, rank, world, local_rank):
             "mean_hits_per_request": mean_hits, "offered_hits_per_s": mean_hits * args.rate,
             "extended_bp_per_s": cells_all / span_all,
             "mean_batch_queries": float(np.mean([o["batch_queries"] for r in runs for o in r["reqs"]])),
-            "rate_sweep": sweep, "gpu_launches": launches, "clocks": clk.summary(),
+            "rate_sweep": sweep, "gpu_launches": launches, "clocks": clk.summary(), "autotune": tuning,
             "setup_s": {"target_generation": t_gen, "load_target": t_load},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "note": "serving is measured end to end; value and e2e are the same measurement"},
@@ -562,6 +582,8 @@ def main():
     ap.add_argument("--tuning", default="", help='JSON of engine launch knobs, e.g. {"gate_tile": 4096}')
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--tune-positions", type=int, default=1 << 24, help="seed positions the autotuner samples")
     ap.add_argument("--rate", type=float, default=50.0, help="config 5: Poisson arrival rate, requests/s")
     ap.add_argument("--requests", type=int, default=32, help="config 5: requests per timed window")
     ap.add_argument("--sweep", default="2,5", help="config 5: extra arrival rates, one window each")

@@ -55,6 +55,15 @@ class QueryC(C.Structure):
     _fields_ = [("ascii", C.c_void_p), ("len", C.c_uint64)]
 
 
+class TuningC(C.Structure):
+    _fields_ = [("gate_tile", C.c_int32), ("gate_cap", C.c_int32), ("gate_blocks_per_sm", C.c_int32),
+                ("graph", C.c_int32), ("best_ms", C.c_double), ("start_ms", C.c_double),
+                ("candidates", C.c_uint32), ("sample_calls", C.c_uint32), ("sample_positions", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServeConfigC(C.Structure):
     _fields_ = [("budget_bytes", C.c_uint64), ("workers", C.c_uint32), ("max_batch_queries", C.c_uint32)]
 
@@ -99,6 +108,7 @@ SIGNATURES = {
     "hz_engine_launches": (U64, [P]),
     "hz_engine_set_stream": (C.c_int, [P, P]),
     "hz_engine_set_tuning": (C.c_int, [P, C.c_char_p, C.c_int64]),
+    "hz_engine_autotune": (C.c_int, [P, U64, C.POINTER(TuningC)]),
     "hz_serve_start": (C.c_int, [P, C.POINTER(ServeConfigC)]),
     "hz_serve_submit": (C.c_int, [P, P, U64, PU64]),
     "hz_serve_poll": (C.c_int, [P, U64, C.c_int, C.POINTER(P), PU64, C.POINTER(ServeTimesC)]),

@@ -208,9 +208,16 @@ class Engine:
 
     def set_tuning(self, **knobs):
         """Launch-shape knobs: gate_tile, gate_cap, gate_blocks_per_sm,
-        wave_positions.  Results never depend on them."""
+        wave_positions, device_dedup, graph.  Results never depend on them."""
         for k, v in knobs.items():
             N.check(N.lib().hz_engine_set_tuning(self._h, k.encode(), int(v)))
+
+    def autotune(self, sample_positions: int = 0) -> dict:
+        """Time candidate launch shapes on a sample of the staged work and keep
+        the fastest (results never depend on them)."""
+        t = N.TuningC()
+        N.check(N.lib().hz_engine_autotune(self._h, int(sample_positions), C.byref(t)))
+        return t.as_dict()
 
     @property
     def launches(self) -> int:

@@ -200,8 +200,30 @@ int hz_engine_profile_reset(hz_engine *e);
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
  * "wave_positions" (seed positions per batched wave), "device_dedup" (1: the
- * batched form dedups on the device, 0: on the host as the plain form does). */
+ * batched form dedups on the device, 0: on the host as the plain form does),
+ * "graph" (1: the batched form captures each wave's kernel chain as a CUDA
+ * graph and replays it, updating the instantiated graph in place). */
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
+
+/* Autotuner (no reference counterpart).  Times the batched form on a
+ * sample of the staged work -- every k-th call, up to sample_positions seed
+ * positions (0 = 2^24) -- under each candidate launch shape and keeps the
+ * fastest: gate_tile (hits staged per gate block: 512..4096, i.e. 16..128
+ * per warp), gate_cap (cells a lane scores before a hit moves to the warp
+ * kernel: 64..1024) and graph (the wave chain replayed as a CUDA graph or
+ * launched kernel by kernel).  Results never depend on the choice. */
+typedef struct hz_tuning {
+  int32_t gate_tile;
+  int32_t gate_cap;
+  int32_t gate_blocks_per_sm;
+  int32_t graph;
+  double best_ms;           /* sample time with the chosen shape */
+  double start_ms;          /* sample time with the shape in place before */
+  uint32_t candidates;
+  uint32_t sample_calls;
+  uint64_t sample_positions;
+} hz_tuning;
+int hz_engine_autotune(hz_engine *e, uint64_t sample_positions, hz_tuning *out);
 
 /* Kernel launches issued by this engine since creation, its serving
  * workers' included. */

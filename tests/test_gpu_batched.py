@@ -60,7 +60,8 @@ def test_batched_equals_plain_per_query(workload):
 @pytest.mark.parametrize("tuning", [dict(wave_positions=50_000), dict(gate_cap=8), dict(gate_cap=4096),
                                     dict(gate_tile=1024, gate_blocks_per_sm=1), dict(gate_tile=4096),
                                     dict(gate_tile=512), dict(device_dedup=0),
-                                    dict(device_dedup=0, wave_positions=5_000)])
+                                    dict(device_dedup=0, wave_positions=5_000), dict(graph=1),
+                                    dict(graph=1, wave_positions=20_000, gate_tile=768)])
 def test_launch_shapes_do_not_change_results(workload, tuning):
     target, chunks = workload
     chunks = chunks[:16]
@@ -97,3 +98,32 @@ def test_empty_and_tiny_queries_in_a_batch(workload):
         got, _ = e.run_batched()
         want = [plain_records(e, q)[0] for q in qs]
     assert per_query(got, len(qs)) == want
+
+
+def test_graph_replay_profiles_and_autotune_keep_results(workload):
+    """The wave chain replayed as a CUDA graph (updated in place from wave to
+    wave) gives the same records; its kernels are still timed one by one; the
+    autotuner picks a valid shape and the results stay identical."""
+    target, chunks = workload
+    chunks = chunks[:20]
+    with Engine(EngineConfig()) as e:
+        e.load_target(target)
+        e.stage_queries(chunks)
+        base, st0 = e.run_batched()
+        e.set_tuning(graph=1, wave_positions=30_000)  # many waves through one instantiated graph
+        e.set_profiling(True)
+        e.profile_reset()
+        got, st1 = e.run_batched()
+        prof = e.profile()
+        e.set_profiling(False)
+        assert got.tobytes() == base.tobytes()
+        assert prof["gate"][1] >= 2 and prof["gate"][0] > 0
+        assert prof["lookup_count"][1] == prof["gate"][1]
+        tune = e.autotune(sample_positions=200_000)
+        assert tune["gate_tile"] in (512, 768, 1024, 2048, 4096)
+        assert tune["gate_cap"] in (64, 128, 256, 512, 1024)
+        assert tune["candidates"] == 50 and tune["sample_calls"] >= 1
+        assert 0 < tune["best_ms"] <= tune["start_ms"]
+        again, st2 = e.run_batched()
+    assert again.tobytes() == base.tobytes()
+    assert (st2["hits"], st2["cells"]) == (st0["hits"], st0["cells"])

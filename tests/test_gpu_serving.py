@@ -29,7 +29,7 @@ def built():
 
 @pytest.fixture(scope="module")
 def workload():
-    return synth.config3(seed=47, scale=0.02, n_chunks=24)
+    return synth.config3(seed=47, scale=0.05, n_chunks=24)
 
 
 def rows(recs):
