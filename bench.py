@@ -579,7 +579,7 @@ def main():
     ap.add_argument("--form", default="both", choices=["both", "batched", "plain"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-batches", type=int, default=80)
-    ap.add_argument("--tuning", default="", help='JSON of engine launch knobs, e.g. {"gate_tile": 4096}')
+    ap.add_argument("--tuning", default="", help='JSON of engine launch knobs, e.g. {"gate_tile": 256}')
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")

@@ -273,7 +273,7 @@ struct hz_engine {
   Slot slot[2];
   // wave buffers
   DBuf<CallDev> calls;
-  DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope, tile_first;
+  DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope, tile_first, tile_call;
   uint32_t tile_cap = 1u << 16;  // entries of the gate's tile table
   DBuf<unsigned long long> np_excl, call_hit_lo, scope_lo;
   DBuf<HitNz> np_partial, np_grand;
@@ -291,7 +291,7 @@ struct hz_engine {
   HBuf<ScopedHspOut> h_out;
   uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
   // tuning
-  int gate_tile = 1024;
+  int gate_tile = 128;  // hits per gate warp tile
   uint32_t gate_cap = 256;
   int gate_blocks_per_sm = 0;
   uint64_t wave_positions = 1ull << 27;  // seed positions per batched wave
@@ -387,26 +387,26 @@ int set_device(hz_engine *e) {
   return HZ_OK;
 }
 
-template <int TILE> size_t gate_smem() { return sizeof(GateSmem<TILE>); }
+template <int TW> size_t gate_smem() { return sizeof(GateSmem<TW>); }
 
-template <int TILE> int launch_gate(hz_engine *e, const GateArgs &ga) {
+template <int TW> int launch_gate(hz_engine *e, const GateArgs &ga) {
   static bool configured[64] = {false};
   static std::mutex mu;  // serving workers launch from several host threads
-  size_t smem = gate_smem<TILE>();
+  size_t smem = gate_smem<TW>();
   {
     std::lock_guard<std::mutex> lock(mu);
     if (!configured[e->device & 63]) {
-      CK(cudaFuncSetAttribute(gate_kernel<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CK(cudaFuncSetAttribute(gate_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       configured[e->device & 63] = true;
     }
   }
   int per_sm = e->gate_blocks_per_sm;
   if (per_sm <= 0) {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate_kernel<TILE>, kScanThreads, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate_kernel<TW>, kGateThreads, smem));
     if (per_sm < 1) per_sm = 1;
   }
   unsigned grid = (unsigned)(e->sm_count * per_sm);
-  return e->launch("gate", [&] { gate_kernel<TILE><<<grid, kScanThreads, smem, e->st>>>(ga); });
+  return e->launch("gate", [&] { gate_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(ga); });
 }
 
 // Runs calls[0..n) as one wave and appends its deduped HSPs, in call order
@@ -582,6 +582,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     TRY(e->raw.ensure(e->raw_cap, s));
     TRY(e->raw_scope.ensure(e->raw_cap, s));
     TRY(e->tile_first.ensure(e->tile_cap, s));
+    TRY(e->tile_call.ensure(e->tile_cap, s));
     // The wave's device chain: no host round trip between its launches, so
     // the batched form can replay it as one CUDA graph.
     auto chain = [&]() -> int {
@@ -603,7 +604,8 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
           4));
       TRY(e->launch("tile_table", [&] {
         tile_table_kernel<<<grid_for(npos, 256, e->sm_count * 8), 256, 0, s>>>(
-            e->np_excl.p, e->pos_hits.p, e->np_pos.p, e->tot.p, (uint32_t)e->gate_tile, e->tile_first.p, e->tile_cap);
+            e->np_excl.p, e->pos_hits.p, e->np_pos.p, e->calls.p, (uint32_t)n, e->tot.p, (uint32_t)e->gate_tile,
+            e->tile_first.p, e->tile_call.p, e->tile_cap);
       }));
       TRY(e->launch("scopes", [&] {
         scopes_kernel<<<1, kScopeThreads, 0, s>>>(w, e->np_excl.p, e->np_pos.p, e->tot.p, e->max_hits,
@@ -624,12 +626,11 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       ga.cand = e->cand.p;
       ga.cand_cap = e->cand_cap;
       ga.tile_first = e->tile_first.p;
+      ga.tile_call = e->tile_call.p;
       switch (e->gate_tile) {
-        case 512: TRY(launch_gate<512>(e, ga)); break;
-        case 768: TRY(launch_gate<768>(e, ga)); break;
-        case 1024: TRY(launch_gate<1024>(e, ga)); break;
-        case 4096: TRY(launch_gate<4096>(e, ga)); break;
-        default: TRY(launch_gate<2048>(e, ga)); break;
+        case 64: TRY(launch_gate<64>(e, ga)); break;
+        case 256: TRY(launch_gate<256>(e, ga)); break;
+        default: TRY(launch_gate<128>(e, ga)); break;
       }
       ExactArgs xa;
       xa.ref = w.ref;
@@ -936,7 +937,7 @@ void hz_engine_destroy(hz_engine *e) {
   e->h_raw_scope.release();
   e->h_scope_call.release();
   for (auto *b : {&e->d_perm_a, &e->d_perm_b, &e->d_keys_a, &e->d_keys_b, &e->d_keep, &e->d_keep_excl, &e->d_hist,
-                  &e->d_hpart, &e->d_total, &e->tile_first})
+                  &e->d_hpart, &e->d_total, &e->tile_first, &e->tile_call})
     b->release();
   e->d_out.release();
   e->h_out.release();
@@ -1530,8 +1531,8 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   if (!e || !key) return fail(HZ_E_INVALID, "null argument");
   std::string k(key);
   if (k == "gate_tile") {
-    if (value != 512 && value != 768 && value != 1024 && value != 2048 && value != 4096)
-      return fail(HZ_E_INVALID, "gate_tile must be 512, 768, 1024, 2048 or 4096");
+    if (value != 64 && value != 128 && value != 256)
+      return fail(HZ_E_INVALID, "gate_tile must be 64, 128 or 256");
     e->gate_tile = (int)value;
   } else if (k == "gate_cap") {
     if (value < 8 || value > 65528 || value % 8) return fail(HZ_E_INVALID, "gate_cap must be a multiple of 8 in 8..65528");
@@ -1578,7 +1579,7 @@ int hz_engine_autotune(hz_engine *e, uint64_t sample_positions, hz_tuning *out) 
   };
   const Knobs start{e->gate_tile, e->gate_cap, e->use_graph};
   std::vector<Knobs> cands;
-  for (int tile : {512, 768, 1024, 2048, 4096})
+  for (int tile : {64, 128, 256})
     for (uint32_t cap : {64u, 128u, 256u, 512u, 1024u})
       for (bool graph : {false, true}) cands.push_back(Knobs{tile, cap, graph});
   bool prof = e->profiling;

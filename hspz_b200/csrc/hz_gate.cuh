@@ -1,20 +1,23 @@
 // Gate kernel of the wave pipeline (included by hz_wave.cuh).
 //
-// A persistent grid takes tiles of consecutive wave hits from a device work
-// queue.  Per tile it
+// A persistent grid of independent warps: each warp takes tiles of TW
+// consecutive wave hits from a device work queue and, with warp-level
+// synchronisation only (no block barrier, so one warp's memory latency in
+// its tile setup overlaps the other warps' scoring),
 //   (1) recomputes the seeds of the positions covering the tile and records
-//       the (position, seed) slots that overlap it;
-//   (2) gives every hit its slot by a block max-scan of slot-start marks and
+//       the (position, seed) slots that overlap it, issuing the bucket
+//       lookups of several seeds at once;
+//   (2) gives every hit its slot by a warp max-scan of slot-start marks and
 //       stores, per hit, the reference and query anchors, the distances to
 //       the sequence edges and the call -- so that a lane picking up a hit
 //       later touches shared memory only;
 //   (3) runs the X-drop score gate thread-per-hit, first all right
-//       extensions and then all left extensions.  Before each pass the block
-//       gathers every hit's first eight cells of both sequences (and the
-//       next word), so a lane's first step needs no global load; each lane
-//       refills from the tile when its extension ends, so extensions of
-//       different lengths do not idle the warp, and it fetches the words of
-//       its next eight cells one step ahead.
+//       extensions of the tile and then all left extensions.  Before each
+//       pass the warp gathers every hit's first eight cells of both
+//       sequences (and the next word), so a lane's first step needs no global
+//       load; each lane refills from the tile when its extension ends, so
+//       extensions of different lengths do not idle the warp, and it fetches
+//       the words of its next eight cells one step ahead.
 // Anchors are the END of the seed window on both sides (pos + seed_size,
 // src/gpu/kernels.rs:397-401).  A hit becomes a candidate when
 // (i32)(f32)(right max + left max) >= hspthresh -- the reference gate's bound
@@ -25,33 +28,37 @@
 
 namespace hz {
 
-// Shared memory of one gate block.  The per-tile setup arrays and the
+constexpr int kGateThreads = 256;
+constexpr int kGateWarps = kGateThreads / 32;
+
+// Shared memory of one warp's tile.  The per-tile setup arrays and the
 // per-pass "first eight cells" arrays are never live at the same time.
-template <int TILE>
-struct GateSmem {
-  int32_t sub[64];
+template <int TW>
+struct WarpTile {
   union {
     struct {
-      uint32_t slot_bst[TILE];  // pos_table index of the slot's first in-tile hit
-      uint32_t slot_q[TILE];    // query anchor (absolute)
-      uint32_t slot_call[TILE];
-      uint32_t hit_slot[TILE];  // first hit of the hit's slot + 1 (mark, then max-scan)
+      uint32_t slot_bst[TW];  // pos_table index of the slot's first in-tile hit
+      uint32_t slot_q[TW];    // query anchor (absolute)
+      uint32_t slot_call[TW];
+      uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
     } setup;
     struct {
-      uint4 first[TILE];   // first eight cells: reference words a, b; query words a, b
-      uint2 carry[TILE];   // the next reference / query word of the stream
+      uint4 first[TW];  // first eight cells: reference words a, b; query words a, b
+      uint2 carry[TW];  // the next reference / query word of the stream
     } pass;
   } u;
-  uint32_t hit_r[TILE];     // reference anchor
-  uint32_t hit_q[TILE];     // query anchor (absolute)
-  uint32_t hit_n[TILE];     // cells to the right edge | cells to the left edge << 16 (each saturated)
-  uint32_t hit_call[TILE];
-  int32_t hit_rmax[TILE];   // right-extension maximum, or kSpilled
-  uint16_t hit_rcells[TILE];
-  uint32_t warp_tot[kScanThreads / 32];
-  unsigned long long h0;
-  uint32_t next, e0, e1, c0;
-  uint32_t next_w[kScanThreads / 32];
+  uint32_t hit_r[TW];     // reference anchor
+  uint32_t hit_q[TW];     // query anchor (absolute)
+  uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
+  uint32_t hit_call[TW];
+  int32_t hit_rmax[TW];   // right-extension maximum, or kSpilled
+  uint16_t hit_rcells[TW];
+};
+
+template <int TW>
+struct GateSmem {
+  int32_t sub[64];
+  WarpTile<TW> warp[kGateWarps];
 };
 constexpr int32_t kSpilled = -1;  // a right maximum is never negative
 
@@ -69,35 +76,31 @@ struct GateArgs {
   Cand *cand;
   uint32_t cand_cap;
   const uint32_t *tile_first;  // first position with hits of each tile (tile_table_kernel)
+  const uint32_t *tile_call;   // call of that position
 };
 
 __device__ __forceinline__ const uint32_t *word_ptr(const uint8_t *p) {
   return reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)3);
 }
 
-// Inclusive max-scan of the slot marks over the tile.
-template <int TILE>
-__device__ __forceinline__ void mark_scan(GateSmem<TILE> &sm, uint32_t nt) {
-  constexpr int PER = TILE / kScanThreads;
-  uint32_t *mark = sm.u.setup.hit_slot;
-  uint32_t base = threadIdx.x * PER;
+// Inclusive max-scan of the slot marks over the warp's tile.
+template <int TW>
+__device__ __forceinline__ void mark_scan(WarpTile<TW> &wt, uint32_t nt, uint32_t lane) {
+  constexpr int PER = TW / 32;
+  uint32_t *mark = wt.u.setup.hit_slot;
+  const uint32_t base = lane * PER;
   uint32_t run = 0;
 #pragma unroll
   for (int i = 0; i < PER; i++)
     if (base + i < nt) run = max(run, mark[base + i]);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t incl = run;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl = max(incl, up);
+    if (lane >= (uint32_t)d) incl = max(incl, up);
   }
-  if (lane == 31) sm.warp_tot[wid] = incl;
-  __syncthreads();
-  uint32_t carry = 0;
-  for (int i = 0; i < wid; i++) carry = max(carry, sm.warp_tot[i]);
-  uint32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
-  if (lane > 0) carry = max(carry, ex);
+  uint32_t carry = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane == 0) carry = 0;
 #pragma unroll
   for (int i = 0; i < PER; i++)
     if (base + i < nt) {
@@ -151,12 +154,11 @@ __device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint
     Smin = min(Smin, S);                                                             \
   }
 
-template <int TILE, bool LEFT>
-__device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm, uint32_t lo, uint32_t hi,
-                                           uint32_t *ctr, unsigned long long &cells_acc) {
+template <int TW, bool LEFT>
+__device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, WarpTile<TW> &wt, uint32_t hi,
+                                           unsigned long long h0, unsigned long long &cells_acc) {
   const uint8_t *ref = a.w.ref;
   const uint8_t *qbuf = a.w.qbuf;
-  const char *subb = reinterpret_cast<const char *>(sm.sub);
   const int32_t X = a.xdrop;
   const uint32_t lane = threadIdx.x & 31;
   bool have = false, exhausted = false, capped = false;
@@ -169,29 +171,28 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
   uint32_t rc = 0, r1 = 0, r2 = 0, qc = 0, q1 = 0, q2 = 0;
   const uint32_t *wr = nullptr, *wq = nullptr;
   uint32_t sr = 0, sq = 0;
+  uint32_t cursor = 0;  // next unclaimed hit of the tile (the same in every lane)
   while (true) {
     if (!exhausted) {
       unsigned need = __ballot_sync(0xffffffffu, !have);
       if (need) {
-        int leader = __ffs(need) - 1;
-        uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(need));
-        base = lo + __shfl_sync(0xffffffffu, base, leader);
-        if (base + __popc(need) >= hi) exhausted = true;
+        const uint32_t base = cursor;
+        cursor += (uint32_t)__popc(need);
+        if (cursor >= hi) exhausted = true;
         if (!have) {
           uint32_t mine = base + __popc(need & lanemask_lt());
-          if (mine < hi && !(LEFT && sm.hit_rmax[mine] == kSpilled)) {
+          if (mine < hi && !(LEFT && wt.hit_rmax[mine] == kSpilled)) {
             have = true;
             t = mine;
-            const uint32_t r0 = sm.hit_r[t], q0 = sm.hit_q[t];
-            n = LEFT ? (sm.hit_n[t] >> 16) : (sm.hit_n[t] & 0xFFFFu);
+            const uint32_t r0 = wt.hit_r[t], q0 = wt.hit_q[t];
+            n = LEFT ? (wt.hit_n[t] >> 16) : (wt.hit_n[t] & 0xFFFFu);
             capped = n > a.cap;
             if (capped) n = a.cap;
             S = 0;
             M = 0;
             cells = 0;
-            uint4 f = sm.u.pass.first[t];
-            uint2 cw = sm.u.pass.carry[t];
+            uint4 f = wt.u.pass.first[t];
+            uint2 cw = wt.u.pass.carry[t];
             ra = f.x;
             rb = f.y;
             qa = f.z;
@@ -301,133 +302,136 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, GateSmem<TILE> &sm
     if (spill) {
       uint32_t at = atomicAdd(&a.tot->cand, 1u);
       if (at < a.cand_cap)
-        a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), sm.hit_r[t],
-                          sm.hit_q[t], sm.hit_call[t] | kLongFlag};
-      if (!LEFT) sm.hit_rmax[t] = kSpilled;  // the left pass skips it
+        a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
+                          wt.hit_q[t], wt.hit_call[t] | kLongFlag};
+      if (!LEFT) wt.hit_rmax[t] = kSpilled;  // the left pass skips it
     } else if (!LEFT) {
-      sm.hit_rmax[t] = res;
-      sm.hit_rcells[t] = (uint16_t)cells;
+      wt.hit_rmax[t] = res;
+      wt.hit_rcells[t] = (uint16_t)cells;
     } else {
-      cells_acc += cells + sm.hit_rcells[t];
-      int32_t total = (int32_t)((uint32_t)sm.hit_rmax[t] + (uint32_t)res);
+      cells_acc += cells + wt.hit_rcells[t];
+      int32_t total = (int32_t)((uint32_t)wt.hit_rmax[t] + (uint32_t)res);
       if (sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
         uint32_t at = atomicAdd(&a.tot->cand, 1u);
         if (at < a.cand_cap)
-          a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), sm.h0 + t), sm.hit_r[t],
-                            sm.hit_q[t], sm.hit_call[t]};
+          a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
+                            wt.hit_q[t], wt.hit_call[t]};
       }
     }
     have = false;
   }
 }
 
-// Fills the first eight cells and the carried word of every hit for one pass.
-template <int TILE, bool LEFT>
-__device__ __forceinline__ void prepare_pass(const GateArgs &a, GateSmem<TILE> &sm, uint32_t lo, uint32_t hi,
-                                             uint32_t first_thread, uint32_t nthreads) {
-  for (uint32_t i = lo + first_thread; i < hi; i += nthreads) {
-    if (LEFT && sm.hit_rmax[i] == kSpilled) continue;
+// Fills the first eight cells and the carried word of every hit of the
+// warp's tile for one pass.
+template <int TW, bool LEFT>
+__device__ __forceinline__ void prepare_pass(const GateArgs &a, WarpTile<TW> &wt, uint32_t nt, uint32_t lane) {
+  for (uint32_t i = lane; i < nt; i += 32) {
+    if (LEFT && wt.hit_rmax[i] == kSpilled) continue;
     uint32_t ra, rb, rc, qa, qb, qc;
-    first_group<LEFT>(a.w.ref, sm.hit_r[i], &ra, &rb, &rc);
-    first_group<LEFT>(a.w.qbuf, sm.hit_q[i], &qa, &qb, &qc);
-    sm.u.pass.first[i] = make_uint4(ra, rb, qa, qb);
-    sm.u.pass.carry[i] = make_uint2(rc, qc);
+    first_group<LEFT>(a.w.ref, wt.hit_r[i], &ra, &rb, &rc);
+    first_group<LEFT>(a.w.qbuf, wt.hit_q[i], &qa, &qb, &qc);
+    wt.u.pass.first[i] = make_uint4(ra, rb, qa, qb);
+    wt.u.pass.carry[i] = make_uint2(rc, qc);
   }
 }
 
-template <int TILE>
-__global__ void __launch_bounds__(kScanThreads) gate_kernel(GateArgs a) {
-  static_assert(TILE % kScanThreads == 0, "tile must be a multiple of the block");
+// Bucket lookups issued per group of seeds, so their loads are in flight
+// together.
+constexpr uint32_t kLookupBatch = 4;
+
+template <int TW>
+__global__ void __launch_bounds__(kGateThreads) gate_kernel(GateArgs a) {
+  static_assert(TW % 32 == 0, "a warp tile is a multiple of 32 hits");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  GateSmem<TILE> &sm = *reinterpret_cast<GateSmem<TILE> *>(smem_raw);
+  GateSmem<TW> &sm = *reinterpret_cast<GateSmem<TW> *>(smem_raw);
   if (a.tot->status & 4u) return;  // no tile table: the host reruns the wave with a larger one
   if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
+  __syncthreads();  // the block's only barrier
+  const char *subb = reinterpret_cast<const char *>(sm.sub);
+  WarpTile<TW> &wt = sm.warp[threadIdx.x >> 5];
+  const uint32_t lane = threadIdx.x & 31;
   unsigned long long cells_acc = 0;
   const unsigned long long total = a.tot->hits;
   const uint32_t nz = a.tot->nz;
   const WaveIn &w = a.w;
   while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) sm.h0 = atomicAdd(&a.tot->tiles, 1ull) * (unsigned long long)TILE;
-    __syncthreads();
-    const unsigned long long h0 = sm.h0;
+    unsigned long long j = 0;
+    if (lane == 0) j = atomicAdd(&a.tot->tiles, 1ull);
+    j = __shfl_sync(0xffffffffu, j, 0);
+    const unsigned long long h0 = j * (unsigned long long)TW;
     if (h0 >= total) break;
-    const uint32_t nt = (uint32_t)min((unsigned long long)TILE, total - h0);
+    const uint32_t nt = (uint32_t)min((unsigned long long)TW, total - h0);
     // positions covering [h0, h0 + nt): the tile table gives the first; the
     // last is the one before the next tile's first, unless that one already
     // started inside this tile
-    if (threadIdx.x == 0) {
-      const uint32_t j = (uint32_t)(h0 / TILE);
-      const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
-      sm.e0 = k0;
-      sm.e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
-      sm.c0 = call_of(w.calls, w.ncalls, a.np_pos[k0]);
-      sm.next = 0;
-    }
-    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) sm.u.setup.hit_slot[i] = 0;
-    __syncthreads();
+    const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
+    const uint32_t e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
+    uint32_t c = a.tile_call[j];  // calls only advance with the position
+    __syncwarp();                 // the previous tile's left pass is done with the union
+    for (uint32_t i = lane; i < nt; i += 32) wt.u.setup.hit_slot[i] = 0;
+    __syncwarp();
     // (1) slots overlapping the tile
-    const uint32_t e0 = sm.e0, e1 = sm.e1;
-    uint32_t c = sm.c0;  // calls only advance with the position
-    for (uint32_t k = e0 + threadIdx.x; k <= e1; k += blockDim.x) {
+    for (uint32_t k = k0 + lane; k <= e1; k += 32) {
       uint32_t p = a.np_pos[k];
       while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
       CallDev cd = w.calls[c];
       uint32_t qpos, kmer;
       position_seed(w, cd, p, &qpos, &kmer);
       unsigned long long lo = a.np_excl[k];
-      for (uint32_t v = 0; v < w.per_pos; v++) {
-        uint32_t beg;
-        uint32_t cnt = bucket(w, seed_variant(kmer, v), &beg);
-        unsigned long long hi = lo + cnt;
-        if (cnt && hi > h0 && lo < h0 + nt) {
-          unsigned long long first = lo > h0 ? lo : h0;
-          uint32_t s = (uint32_t)(first - h0);
-          sm.u.setup.slot_bst[s] = beg + (uint32_t)(first - lo);
-          sm.u.setup.slot_q[s] = cd.qoff + qpos + w.shape.size;
-          sm.u.setup.slot_call[s] = c;
-          sm.u.setup.hit_slot[s] = s + 1;
+      const uint32_t q_anchor = cd.qoff + qpos + w.shape.size;
+      for (uint32_t v0 = 0; v0 < w.per_pos; v0 += kLookupBatch) {
+        uint32_t beg[kLookupBatch], cnt[kLookupBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kLookupBatch; u++) {
+          cnt[u] = 0;
+          beg[u] = 0;
+          if (v0 + u < w.per_pos) cnt[u] = bucket(w, seed_variant(kmer, v0 + u), &beg[u]);
         }
-        lo = hi;
+#pragma unroll
+        for (uint32_t u = 0; u < kLookupBatch; u++) {
+          unsigned long long hi = lo + cnt[u];
+          if (cnt[u] && hi > h0 && lo < h0 + nt) {
+            unsigned long long first = lo > h0 ? lo : h0;
+            uint32_t s = (uint32_t)(first - h0);
+            wt.u.setup.slot_bst[s] = beg[u] + (uint32_t)(first - lo);
+            wt.u.setup.slot_q[s] = q_anchor;
+            wt.u.setup.slot_call[s] = c;
+            wt.u.setup.hit_slot[s] = s + 1;
+          }
+          lo = hi;
+        }
       }
     }
-    __syncthreads();
+    __syncwarp();
     // (2) per hit: slot, anchors, edge distances, call
-    mark_scan<TILE>(sm, nt);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-      uint32_t s = sm.u.setup.hit_slot[i] - 1;
-      uint32_t r0 = __ldg(w.pos_table + sm.u.setup.slot_bst[s] + (i - s)) + w.shape.size;
-      uint32_t q0 = sm.u.setup.slot_q[s];
-      uint32_t c = sm.u.setup.slot_call[s];
-      const CallDev &cd = w.calls[c];
+    mark_scan<TW>(wt, nt, lane);
+    __syncwarp();
+    for (uint32_t i = lane; i < nt; i += 32) {
+      uint32_t s = wt.u.setup.hit_slot[i] - 1;
+      uint32_t r0 = __ldg(w.pos_table + wt.u.setup.slot_bst[s] + (i - s)) + w.shape.size;
+      uint32_t q0 = wt.u.setup.slot_q[s];
+      uint32_t hc = wt.u.setup.slot_call[s];
+      const CallDev &cd = w.calls[hc];
       uint32_t nr = min(w.rlen - r0, cd.qoff + cd.qlen - q0);
       uint32_t nl = min(r0, q0 - cd.qoff);
-      sm.hit_r[i] = r0;
-      sm.hit_q[i] = q0;
-      sm.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
-      sm.hit_call[i] = c;
+      wt.hit_r[i] = r0;
+      wt.hit_q[i] = q0;
+      wt.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
+      wt.hit_call[i] = hc;
     }
-    __syncthreads();
+    __syncwarp();
     // (3) the score gate: right pass, then left pass
-    prepare_pass<TILE, false>(a, sm, 0, nt, threadIdx.x, blockDim.x);
-    __syncthreads();
-    {
-      // each warp takes a fixed slice of the tile through both passes
-      const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-      const uint32_t lo = (uint32_t)((uint64_t)nt * wid / nw), hi = (uint32_t)((uint64_t)nt * (wid + 1) / nw);
-      if (lane == 0) sm.next_w[wid] = 0;
-      __syncwarp();
-      gate_phase<TILE, false>(a, sm, lo, hi, &sm.next_w[wid], cells_acc);
-      __syncwarp();
-      if (lane == 0) sm.next_w[wid] = 0;
-      prepare_pass<TILE, true>(a, sm, lo, hi, lane, 32);
-      __syncwarp();
-      gate_phase<TILE, true>(a, sm, lo, hi, &sm.next_w[wid], cells_acc);
-    }
+    prepare_pass<TW, false>(a, wt, nt, lane);
+    __syncwarp();
+    gate_phase<TW, false>(a, subb, wt, nt, h0, cells_acc);
+    __syncwarp();
+    prepare_pass<TW, true>(a, wt, nt, lane);
+    __syncwarp();
+    gate_phase<TW, true>(a, subb, wt, nt, h0, cells_acc);
   }
   for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
-  if ((threadIdx.x & 31) == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
+  if (lane == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
 }
 
 }  // namespace hz

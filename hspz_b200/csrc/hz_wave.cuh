@@ -203,12 +203,14 @@ __global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *_
 
 // The gate's tile table: tile_first[j] = the position with hits that holds
 // wave hit j * tile (positions tile the hit space, so every tile start has
-// exactly one), and tile_first[n_tiles] = nz.  Lets a gate block find its
-// positions with two loads instead of a search.  Sets status bit 2 when the
+// exactly one), tile_call[j] = the call of that position, and
+// tile_first[n_tiles] = nz.  Lets a gate warp find its positions and call
+// with three loads instead of searches.  Sets status bit 2 when the
 // table is too small (the wave is then rerun with a larger one).
 __global__ void tile_table_kernel(const unsigned long long *__restrict__ np_excl, const uint32_t *__restrict__ pos_hits,
-                                  const uint32_t *__restrict__ np_pos, WaveTotals *__restrict__ t, uint32_t tile,
-                                  uint32_t *__restrict__ tile_first, uint32_t cap) {
+                                  const uint32_t *__restrict__ np_pos, const CallDev *__restrict__ calls,
+                                  uint32_t ncalls, WaveTotals *__restrict__ t, uint32_t tile,
+                                  uint32_t *__restrict__ tile_first, uint32_t *__restrict__ tile_call, uint32_t cap) {
   const uint32_t nz = t->nz;
   const unsigned long long total = t->hits;
   const unsigned long long n_tiles = (total + tile - 1) / tile;
@@ -218,8 +220,15 @@ __global__ void tile_table_kernel(const unsigned long long *__restrict__ np_excl
   }
   uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nz; k += stride) {
-    unsigned long long lo = np_excl[k], hi = lo + pos_hits[np_pos[k]];
-    for (unsigned long long j = (lo + tile - 1) / tile; j * tile < hi; j++) tile_first[j] = k;
+    const uint32_t p = np_pos[k];
+    unsigned long long lo = np_excl[k], hi = lo + pos_hits[p];
+    unsigned long long j = (lo + tile - 1) / tile;
+    if (j * tile >= hi) continue;
+    const uint32_t c = call_of(calls, ncalls, p);
+    for (; j * tile < hi; j++) {
+      tile_first[j] = k;
+      tile_call[j] = c;
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) tile_first[n_tiles] = nz;
 }

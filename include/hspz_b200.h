@@ -196,7 +196,7 @@ int hz_engine_profile_entry(hz_engine *e, uint32_t i, char *name, uint32_t name_
 int hz_engine_profile_reset(hz_engine *e);
 
 /* Launch-shape knobs (no reference counterpart; results never depend on
- * them): "gate_tile" (hits per gate block tile: 512, 768, 1024, 2048, 4096),
+ * them): "gate_tile" (hits per gate warp tile: 64, 128, 256),
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
  * "wave_positions" (seed positions per batched wave), "device_dedup" (1: the
@@ -208,8 +208,8 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
 /* Autotuner (no reference counterpart).  Times the batched form on a
  * sample of the staged work -- every k-th call, up to sample_positions seed
  * positions (0 = 2^24) -- under each candidate launch shape and keeps the
- * fastest: gate_tile (hits staged per gate block: 512..4096, i.e. 16..128
- * per warp), gate_cap (cells a lane scores before a hit moves to the warp
+ * fastest: gate_tile (hits a gate warp stages per tile: 64, 128, 256, i.e.
+ * 2..8 per lane), gate_cap (cells a lane scores before a hit moves to the warp
  * kernel: 64..1024) and graph (the wave chain replayed as a CUDA graph or
  * launched kernel by kernel).  Results never depend on the choice. */
 typedef struct hz_tuning {
