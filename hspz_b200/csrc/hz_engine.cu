@@ -219,25 +219,9 @@ struct HostCall {
 };
 
 // A staged query block: forward and reverse-complement codes in the store.
-// One staged query block in the query store: the forward and reverse-
-// complement strands, and each strand reversed (the gate runs left
-// extensions as right extensions over the reversed copies).
 struct StagedQuery {
-  uint32_t off_f = 0, off_r = 0, off_fr = 0, off_rr = 0, len = 0;
+  uint32_t off_f = 0, off_r = 0, len = 0;
 };
-
-// Appends a query block of `len` bases to a store layout of *total bytes:
-// four strands, each 16-byte aligned with at least kPad bytes after it.
-inline StagedQuery layout_query(uint64_t len, uint64_t *total) {
-  StagedQuery q;
-  q.len = (uint32_t)len;
-  uint32_t *offs[4] = {&q.off_f, &q.off_r, &q.off_fr, &q.off_rr};
-  for (uint32_t *o : offs) {
-    *o = (uint32_t)*total;
-    *total = (*total + len + kPad + 15) & ~15ull;
-  }
-  return q;
-}
 
 struct Slot {
   int kind = 0;  // 0 empty, 1 uploaded seeds, 2 generated range
@@ -272,7 +256,6 @@ struct hz_engine {
   uint32_t max_hits = 0;
   // target
   SeqBuf ref;
-  SeqBuf ref_rev;  // the reference reversed (left extensions run over it)
   uint32_t rlen = 0;
   DBuf<uint32_t> index_table;
   uint64_t index_len = 0;
@@ -557,7 +540,6 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     const StagedQuery &q = e->queries[hc[i].query];
     CallDev &c = e->h_calls.p[i];
     c.qoff = hc[i].strand ? q.off_r : q.off_f;
-    c.qoff_rev = hc[i].strand ? q.off_rr : q.off_fr;
     c.qlen = q.len;
     c.start = hc[i].start;
     c.pos_off = (uint32_t)npos;
@@ -580,7 +562,6 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
 
   WaveIn w;
   w.ref = e->ref.base();
-  w.ref_rev = e->ref_rev.base();
   w.rlen = e->rlen;
   w.qbuf = e->qstore.base();
   w.index_table = e->index_table.p;
@@ -758,27 +739,6 @@ void query_calls(const hz_engine *e, uint32_t qid, std::vector<HostCall> *out) {
   }
 }
 
-// The reversed reference beside the reference codes.
-int reverse_ref(hz_engine *e, uint64_t len) {
-  TRY(e->ref_rev.ensure(len, e->st));
-  if (!len) return HZ_OK;
-  const uint8_t *src = e->ref.base();
-  uint8_t *dst = e->ref_rev.base();
-  cudaStream_t s = e->st;
-  return e->launch("reverse", [&] { reverse_kernel<<<grid_for(len, 256), 256, 0, s>>>(src, len, dst); });
-}
-
-// Writes the reversed copies of a staged query's two strands.
-int reverse_strands(hz_engine *e, const StagedQuery &q) {
-  if (!q.len) return HZ_OK;
-  uint8_t *base = e->qstore.base();
-  cudaStream_t s = e->st;
-  return e->launch("reverse", [&] {
-    reverse_kernel<<<grid_for(q.len, 256), 256, 0, s>>>(base + q.off_f, q.len, base + q.off_fr);
-    reverse_kernel<<<grid_for(q.len, 256), 256, 0, s>>>(base + q.off_r, q.len, base + q.off_rr);
-  }, 2);
-}
-
 // Replaces the query store with `nq` ASCII blocks; each is encoded forward
 // and reverse-complemented on the device.
 int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens, uint32_t nq) {
@@ -786,7 +746,12 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
   std::vector<StagedQuery> qs(nq);
   for (uint32_t i = 0; i < nq; i++) {
     if (lens[i] > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "query block %u exceeds u32 coordinates", i);
-    qs[i] = layout_query(lens[i], &total);
+    // every strand starts 16-byte aligned, with at least kPad bytes after it
+    qs[i].len = (uint32_t)lens[i];
+    qs[i].off_f = (uint32_t)total;
+    total = (total + lens[i] + kPad + 15) & ~15ull;
+    qs[i].off_r = (uint32_t)total;
+    total = (total + lens[i] + kPad + 15) & ~15ull;
   }
   if (total >= 0xFFFFFFFFull) return fail(HZ_E_INVALID, "staged queries exceed 4 GB");
   cudaStream_t s = e->st;
@@ -803,7 +768,6 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
     TRY(e->launch("encode", [&] {
       encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, s>>>(e->qascii.p, len, f, r);
     }));
-    TRY(reverse_strands(e, qs[i]));
   }
   TRY(e->sync());
   e->queries = qs;
@@ -931,7 +895,6 @@ int hz_engine_create(const hz_config *cfg, int device, hz_engine **out) {
   if (cudaMemcpyToSymbol(c_enc, t_enc, 256) != cudaSuccess || cudaMemcpyToSymbol(c_enc_rc, t_rc, 256) != cudaSuccess)
     rc = fail(HZ_E_CUDA, "constant tables: %s", cudaGetErrorString(cudaGetLastError()));
   if (rc == HZ_OK) rc = e->ref.ensure(0, e->st);
-  if (rc == HZ_OK) rc = e->ref_rev.ensure(0, e->st);
   if (rc == HZ_OK) rc = e->qstore.ensure(0, e->st);
   if (rc != HZ_OK) {
     hz_engine_destroy(e);
@@ -948,7 +911,6 @@ void hz_engine_destroy(hz_engine *e) {
   if (e->server) hz_serve_stop(e);
   if (e->owns_target) {
     e->ref.buf.release();
-    e->ref_rev.buf.release();
     e->index_table.release();
     e->pos_table.release();
   }
@@ -1024,7 +986,6 @@ int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t in
   CK(cudaMemcpyAsync(e->index_table.p, index_table, index_len * 4, cudaMemcpyHostToDevice, s));
   if (pos_len) CK(cudaMemcpyAsync(e->pos_table.p, pos_table, pos_len * 4, cudaMemcpyHostToDevice, s));
   if (ref_len) CK(cudaMemcpyAsync(e->ref.base(), ref_seq, ref_len, cudaMemcpyHostToDevice, s));
-  TRY(reverse_ref(e, ref_len));
   TRY(e->sync());
   e->index_len = index_len;
   e->n_pos = pos_len;
@@ -1057,7 +1018,6 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
     TRY(e->launch("encode", [&] {
       encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, st>>>(ascii.p, len, codes, junk.p);
     }));
-  TRY(reverse_ref(e, len));
   TRY(e->index_table.ensure(index_len, st));
   CK(cudaMemsetAsync(e->index_table.p, 0, index_len * 4, st));
 
@@ -1166,14 +1126,16 @@ int hz_swap_query(hz_engine *e, const uint8_t *query, const uint8_t *query_rc, u
   for (uint64_t i = 0; i < len; i++)
     if (query[i] > 7 || query_rc[i] > 7) return fail(HZ_E_INVALID, "query byte %llu is not a device-alphabet code", (unsigned long long)i);
   TRY(set_device(e));
-  uint64_t total = 0;
-  StagedQuery q = layout_query(len, &total);
+  StagedQuery q;
+  q.len = (uint32_t)len;
+  q.off_f = 0;
+  q.off_r = (uint32_t)((len + kPad + 15) & ~15ull);
+  uint64_t total = q.off_r + len + kPad;
   TRY(e->qstore.ensure(total, e->st));
   CK(cudaMemsetAsync(e->qstore.base(), 0, total, e->st));
   if (len) {
     CK(cudaMemcpyAsync(e->qstore.base() + q.off_f, query, len, cudaMemcpyHostToDevice, e->st));
     CK(cudaMemcpyAsync(e->qstore.base() + q.off_r, query_rc, len, cudaMemcpyHostToDevice, e->st));
-    TRY(reverse_strands(e, q));
   }
   TRY(e->sync());
   e->queries.assign(1, q);
@@ -1231,7 +1193,7 @@ int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint
     // the lookup kernel counts valid windows as it goes: run it alone
     const StagedQuery &q = e->queries[e->cur_query];
     TRY(e->h_calls.ensure(1));
-    e->h_calls.p[0] = CallDev{s.rev ? q.off_r : q.off_f, q.len, start, 0, s.rev ? q.off_rr : q.off_fr};
+    e->h_calls.p[0] = CallDev{s.rev ? q.off_r : q.off_f, q.len, start, 0};
     TRY(e->calls.ensure(1, e->st));
     TRY(e->pos_hits.ensure(end - start, e->st));
     TRY(e->tot.ensure(1, e->st));
@@ -1750,9 +1712,6 @@ int clone_shared(hz_engine *e, hz_engine **out) {
   w->ref.buf.p = e->ref.buf.p;
   w->ref.buf.cap = e->ref.buf.cap;
   w->ref.len = e->ref.len;
-  w->ref_rev.buf.p = e->ref_rev.buf.p;
-  w->ref_rev.buf.cap = e->ref_rev.buf.cap;
-  w->ref_rev.len = e->ref_rev.len;
   w->rlen = e->rlen;
   w->index_table.p = e->index_table.p;
   w->index_table.cap = e->index_table.cap;

@@ -9,16 +9,15 @@
 //       lookups of several seeds at once;
 //   (2) gives every hit its slot by a warp max-scan of slot-start marks and
 //       stores, per hit, the reference and query anchors, the distances to
-//       the sequence edges and the call, plus the first eight cells of both
-//       extensions -- so that a lane picking up a hit touches shared memory
-//       only;
-//   (3) runs the X-drop score gate thread-per-hit: a lane scores a hit's
-//       right extension and then its left extension, and takes the next hit
-//       of the tile when both end, so extensions of different lengths do
-//       not idle the warp.  A left extension is scored as a right extension
-//       over the reversed reference and query copies, so both directions
-//       run the same code: eight cells per step from two 4-byte words per
-//       sequence, the words of the next step fetched one step ahead.
+//       the sequence edges and the call -- so that a lane picking up a hit
+//       later touches shared memory only;
+//   (3) runs the X-drop score gate thread-per-hit, first all right
+//       extensions of the tile and then all left extensions.  Before each
+//       pass the warp gathers every hit's first eight cells of both
+//       sequences (and the next word), so a lane's first step needs no global
+//       load; each lane refills from the tile when its extension ends, so
+//       extensions of different lengths do not idle the warp, and it fetches
+//       the words of its next eight cells one step ahead.
 // Anchors are the END of the seed window on both sides (pos + seed_size,
 // src/gpu/kernels.rs:397-401).  A hit becomes a candidate when
 // (i32)(f32)(right max + left max) >= hspthresh -- the reference gate's bound
@@ -33,7 +32,7 @@ constexpr int kGateThreads = 256;
 constexpr int kGateWarps = kGateThreads / 32;
 
 // Shared memory of one warp's tile.  The per-tile setup arrays and the
-// first cells of the extensions are never live at the same time.
+// per-pass "first eight cells" arrays are never live at the same time.
 template <int TW>
 struct WarpTile {
   union {
@@ -44,15 +43,16 @@ struct WarpTile {
       uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
     } setup;
     struct {
-      uint4 right[TW];  // first eight cells to the right: reference words a, b; query words a, b
-      uint4 left[TW];   // the same to the left, from the reversed copies
+      uint4 first[TW];  // first eight cells: reference words a, b; query words a, b
+      uint2 carry[TW];  // the next reference / query word of the stream
     } pass;
   } u;
-  uint32_t hit_r[TW];   // reference anchor
-  uint32_t hit_q[TW];   // query anchor (absolute)
-  uint32_t hit_ql[TW];  // query anchor in the reversed copy of the strand
-  uint32_t hit_n[TW];   // cells to the right edge | cells to the left edge << 16 (each saturated)
+  uint32_t hit_r[TW];     // reference anchor
+  uint32_t hit_q[TW];     // query anchor (absolute)
+  uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
   uint32_t hit_call[TW];
+  int32_t hit_rmax[TW];   // right-extension maximum, or kSpilled
+  uint16_t hit_rcells[TW];
 };
 
 template <int TW>
@@ -60,6 +60,7 @@ struct GateSmem {
   int32_t sub[64];
   WarpTile<TW> warp[kGateWarps];
 };
+constexpr int32_t kSpilled = -1;  // a right maximum is never negative
 
 struct GateArgs {
   WaveIn w;
@@ -118,143 +119,173 @@ __device__ __forceinline__ uint32_t scope_of(const unsigned long long *scope_lo,
   return lo;
 }
 
-// The eight bytes [p, p+8) as two words, cell 0 in the low byte.
-__device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint32_t *a, uint32_t *b) {
+// The eight bytes [p, p+8) (right) or [p-8, p) reversed (left) as two words,
+// cell 0 in the low byte, plus the word the next step continues from.
+template <bool LEFT>
+__device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint32_t *a, uint32_t *b,
+                                            uint32_t *carry) {
   const uint32_t sh = (p & 3u) * 8u;
-  const uint32_t *w = word_ptr(seq + p);
-  uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
-  *a = __funnelshift_r(w0, w1, sh);
-  *b = __funnelshift_r(w1, w2, sh);
+  if (!LEFT) {
+    const uint32_t *w = word_ptr(seq + p);
+    uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+    *a = __funnelshift_r(w0, w1, sh);
+    *b = __funnelshift_r(w1, w2, sh);
+    *carry = w2;
+  } else {
+    const uint32_t *w = word_ptr(seq + p - 8);
+    uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+    *a = __byte_perm(__funnelshift_r(w1, w2, sh), 0, 0x0123);
+    *b = __byte_perm(__funnelshift_r(w0, w1, sh), 0, 0x0123);
+    *carry = w0;
+  }
 }
 
-// Scores the two cells whose byte offsets into the substitution table are
-// bytes SH0 and SH1 of T: the running sums after each go to Si[I], Si[I+1];
-// the group's running maximum M and smallest sum Smin take both at once.
-// Since every cell's maximum is <= the group's final M, no cell of the group
-// can have dropped when M - Smin <= xdrop.
-#define HZ_PAIR(T, SH0, SH1, I)                                                            \
-  {                                                                                        \
-    const int32_t s0 = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH0)) & 0xFFu)); \
-    const int32_t s1 = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH1)) & 0xFFu)); \
-    Si[I] = (int32_t)((uint32_t)S + (uint32_t)s0);                                         \
-    S = (int32_t)((uint32_t)Si[I] + (uint32_t)s1);                                         \
-    Si[I + 1] = S;                                                                         \
-    M = __vimax3_s32(M, Si[I], S);                                                         \
-    Smin = __vimin3_s32(Smin, Si[I], S);                                                   \
+// Scores one cell whose byte offset into the substitution table is byte SH
+// of T; keeps every running sum S and maximum M for the termination path
+// and the group's smallest sum. Since every M_i <= M_7, no cell of the group
+// can have dropped when M_7 - min S <= xdrop.
+#define HZ_CELL(T, SH, I)                                                            \
+  {                                                                                  \
+    int32_t sc = *reinterpret_cast<const int32_t *>(subb + (((T) >> (SH)) & 0xFFu)); \
+    S = (int32_t)((uint32_t)S + (uint32_t)sc);                                       \
+    M = max(M, S);                                                                   \
+    Si[I] = S;                                                                       \
+    Mi[I] = M;                                                                       \
+    Smin = min(Smin, S);                                                             \
   }
 
-// Stream state of one lane's extension: the group about to be scored (ra,
-// rb, qa, qb), the carried word and the two prefetched words of each
-// sequence, and where the next words come from.
-struct Stream {
-  uint32_t ra, rb, qa, qb;
-  uint32_t rc, r1, r2, qc, q1, q2;
-  const uint32_t *wr, *wq;
-  uint32_t sr, sq;
-};
-
-// Starts a stream at reference position pr of `rseq` and query position pq
-// of `qseq`, given the first group's words.
-__device__ __forceinline__ void stream_begin(Stream &st, const uint8_t *rseq, uint32_t pr, const uint8_t *qseq,
-                                             uint32_t pq, uint4 f) {
-  st.ra = f.x;
-  st.rb = f.y;
-  st.qa = f.z;
-  st.qb = f.w;
-  st.sr = (pr & 3u) * 8u;
-  st.sq = (pq & 3u) * 8u;
-  st.wr = word_ptr(rseq + pr) + 2;  // the carried word
-  st.wq = word_ptr(qseq + pq) + 2;
-  st.rc = __ldg(st.wr);
-  st.r1 = __ldg(st.wr + 1);
-  st.r2 = __ldg(st.wr + 2);
-  st.qc = __ldg(st.wq);
-  st.q1 = __ldg(st.wq + 1);
-  st.q2 = __ldg(st.wq + 2);
-}
-
-// The thread-per-hit gate over the warp's tile of nt hits.
-template <int TW>
-__device__ __forceinline__ void gate_run(const GateArgs &a, const char *subb, WarpTile<TW> &wt, uint32_t nt,
-                                         unsigned long long h0, unsigned long long &cells_acc) {
-  const uint8_t *ref = a.w.ref, *ref_rev = a.w.ref_rev, *qbuf = a.w.qbuf;
+template <int TW, bool LEFT>
+__device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, WarpTile<TW> &wt, uint32_t hi,
+                                           unsigned long long h0, unsigned long long &cells_acc) {
+  const uint8_t *ref = a.w.ref;
+  const uint8_t *qbuf = a.w.qbuf;
   const int32_t X = a.xdrop;
   const uint32_t lane = threadIdx.x & 31;
-  bool have = false, exhausted = false, second = false, capped = false;
-  uint32_t t = 0, n = 0, cells = 0, cells_r = 0;
-  int32_t S = 0, M = 0, rmax = 0;
-  Stream st;
-  st.wr = st.wq = nullptr;
-  st.ra = st.rb = st.qa = st.qb = st.rc = st.r1 = st.r2 = st.qc = st.q1 = st.q2 = st.sr = st.sq = 0;
+  bool have = false, exhausted = false, capped = false;
+  uint32_t t = 0, n = 0;
+  int32_t S = 0, M = 0;
+  uint32_t cells = 0;
+  // word stream state: the group about to be scored (ra, rb, qa, qb), the
+  // carried word and the two prefetched words of the following group
+  uint32_t ra = 0, rb = 0, qa = 0, qb = 0;
+  uint32_t rc = 0, r1 = 0, r2 = 0, qc = 0, q1 = 0, q2 = 0;
+  const uint32_t *wr = nullptr, *wq = nullptr;
+  uint32_t sr = 0, sq = 0;
   uint32_t cursor = 0;  // next unclaimed hit of the tile (the same in every lane)
   while (true) {
     if (!exhausted) {
-      const unsigned need = __ballot_sync(0xffffffffu, !have);
+      unsigned need = __ballot_sync(0xffffffffu, !have);
       if (need) {
         const uint32_t base = cursor;
         cursor += (uint32_t)__popc(need);
-        if (cursor >= nt) exhausted = true;
+        if (cursor >= hi) exhausted = true;
         if (!have) {
-          const uint32_t mine = base + __popc(need & lanemask_lt());
-          if (mine < nt) {
+          uint32_t mine = base + __popc(need & lanemask_lt());
+          if (mine < hi && !(LEFT && wt.hit_rmax[mine] == kSpilled)) {
             have = true;
-            second = false;
             t = mine;
-            const uint32_t nr = wt.hit_n[t] & 0xFFFFu;
-            capped = nr > a.cap;
-            n = capped ? a.cap : nr;
-            S = M = 0;
+            const uint32_t r0 = wt.hit_r[t], q0 = wt.hit_q[t];
+            n = LEFT ? (wt.hit_n[t] >> 16) : (wt.hit_n[t] & 0xFFFFu);
+            capped = n > a.cap;
+            if (capped) n = a.cap;
+            S = 0;
+            M = 0;
             cells = 0;
-            stream_begin(st, ref, wt.hit_r[t], qbuf, wt.hit_q[t], wt.u.pass.right[t]);
+            uint4 f = wt.u.pass.first[t];
+            uint2 cw = wt.u.pass.carry[t];
+            ra = f.x;
+            rb = f.y;
+            qa = f.z;
+            qb = f.w;
+            rc = cw.x;
+            qc = cw.y;
+            sr = (r0 & 3u) * 8u;
+            sq = (q0 & 3u) * 8u;
+            if (!LEFT) {
+              wr = word_ptr(ref + r0) + 2;  // the carried word
+              wq = word_ptr(qbuf + q0) + 2;
+              r1 = __ldg(wr + 1);
+              r2 = __ldg(wr + 2);
+              q1 = __ldg(wq + 1);
+              q2 = __ldg(wq + 2);
+            } else {
+              wr = word_ptr(ref + r0 - 8);  // the carried word
+              wq = word_ptr(qbuf + q0 - 8);
+              r1 = __ldg(wr - 1);
+              r2 = __ldg(wr - 2);
+              q1 = __ldg(wq - 1);
+              q2 = __ldg(wq - 2);
+            }
           }
         }
       }
     }
+    // (in the left pass a refill may hand out only hits that were spilled in
+    // the right pass, so an idle warp ends only once the tile is exhausted)
     if (!__any_sync(0xffffffffu, have) && exhausted) break;
     if (!have) continue;
     // ---- eight cells ----
     // codes are 0..7, so (r << 5) | (q << 2) is the byte offset of sub[r*8+q]
-    const uint32_t ta = (st.ra << 5) | (st.qa << 2), tb = (st.rb << 5) | (st.qb << 2);
-    // the next group from the carried and prefetched words
-    const uint32_t nra = __funnelshift_r(st.rc, st.r1, st.sr), nrb = __funnelshift_r(st.r1, st.r2, st.sr);
-    const uint32_t nqa = __funnelshift_r(st.qc, st.q1, st.sq), nqb = __funnelshift_r(st.q1, st.q2, st.sq);
+    const uint32_t ta = (ra << 5) | (qa << 2), tb = (rb << 5) | (qb << 2);
+    // the next group from the carried and prefetched words; prefetch again
+    uint32_t nra, nrb, nqa, nqb;
+    if (!LEFT) {
+      nra = __funnelshift_r(rc, r1, sr);
+      nrb = __funnelshift_r(r1, r2, sr);
+      nqa = __funnelshift_r(qc, q1, sq);
+      nqb = __funnelshift_r(q1, q2, sq);
+      rc = r2;
+      qc = q2;
+      wr += 2;
+      wq += 2;
+    } else {
+      nra = __byte_perm(__funnelshift_r(r1, rc, sr), 0, 0x0123);
+      nrb = __byte_perm(__funnelshift_r(r2, r1, sr), 0, 0x0123);
+      nqa = __byte_perm(__funnelshift_r(q1, qc, sq), 0, 0x0123);
+      nqb = __byte_perm(__funnelshift_r(q2, q1, sq), 0, 0x0123);
+      rc = r2;
+      qc = q2;
+      wr -= 2;
+      wq -= 2;
+    }
     const int32_t Ms = M;
-    int32_t Si[8];
+    int32_t Si[8], Mi[8];
     int32_t Smin = S;
-    HZ_PAIR(ta, 0, 8, 0)
-    HZ_PAIR(ta, 16, 24, 2)
-    HZ_PAIR(tb, 0, 8, 4)
-    HZ_PAIR(tb, 16, 24, 6)
-    // first valid cell with M_i - S_i > xdrop, if the bound says there may be one
+    HZ_CELL(ta, 0, 0)
+    HZ_CELL(ta, 8, 1)
+    HZ_CELL(ta, 16, 2)
+    HZ_CELL(ta, 24, 3)
+    HZ_CELL(tb, 0, 4)
+    HZ_CELL(tb, 8, 5)
+    HZ_CELL(tb, 16, 6)
+    HZ_CELL(tb, 24, 7)
+    // first valid cell with M - S > xdrop, if the bound says there may be one
     const uint32_t v = min(n, 8u);
     uint32_t dm = 0;
-    int32_t Mi[8];
     if ((int32_t)((uint32_t)M - (uint32_t)Smin) > X || n <= 8) {
-      int32_t m = Ms;
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
-        m = max(m, Si[i]);
-        Mi[i] = m;
-        dm |= (uint32_t)((int32_t)((uint32_t)m - (uint32_t)Si[i]) > X) << i;
-      }
+      for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
       dm &= (1u << v) - 1u;
     }
     if (!dm && n > 8) {  // no drop and more cells left: advance the stream
       n -= 8;
       cells += 8;
-      st.ra = nra;
-      st.rb = nrb;
-      st.qa = nqa;
-      st.qb = nqb;
-      st.rc = st.r2;
-      st.qc = st.q2;
-      st.wr += 2;
-      st.wq += 2;
+      ra = nra;
+      rb = nrb;
+      qa = nqa;
+      qb = nqb;
       if (n > 8) {  // words of the group after next (never beyond the padding)
-        st.r1 = __ldg(st.wr + 1);
-        st.r2 = __ldg(st.wr + 2);
-        st.q1 = __ldg(st.wq + 1);
-        st.q2 = __ldg(st.wq + 2);
+        if (!LEFT) {
+          r1 = __ldg(wr + 1);
+          r2 = __ldg(wr + 2);
+          q1 = __ldg(wq + 1);
+          q2 = __ldg(wq + 2);
+        } else {
+          r1 = __ldg(wr - 1);
+          r2 = __ldg(wr - 2);
+          q1 = __ldg(wq - 1);
+          q2 = __ldg(wq - 2);
+        }
       }
       continue;
     }
@@ -267,49 +298,41 @@ __device__ __forceinline__ void gate_run(const GateArgs &a, const char *subb, Wa
     for (int i = 1; i <= 8; i++)
       if ((uint32_t)i == stop) res = Mi[i - 1];
     cells += dm ? stop + 1 : v;
-    if (!dm && capped) {  // long: the exact kernel redoes the hit; its cells are counted there
+    const bool spill = !dm && capped;
+    if (spill) {
       uint32_t at = atomicAdd(&a.tot->cand, 1u);
       if (at < a.cand_cap)
         a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
                           wt.hit_q[t], wt.hit_call[t] | kLongFlag};
-      have = false;
-    } else if (!second) {  // the right extension ended: start the left one
-      rmax = res;
-      cells_r = cells;
-      second = true;
-      const uint32_t nl = wt.hit_n[t] >> 16;
-      capped = nl > a.cap;
-      n = capped ? a.cap : nl;
-      S = M = 0;
-      cells = 0;
-      stream_begin(st, ref_rev, a.w.rlen - wt.hit_r[t], qbuf, wt.hit_ql[t], wt.u.pass.left[t]);
+      if (!LEFT) wt.hit_rmax[t] = kSpilled;  // the left pass skips it
+    } else if (!LEFT) {
+      wt.hit_rmax[t] = res;
+      wt.hit_rcells[t] = (uint16_t)cells;
     } else {
-      cells_acc += cells + cells_r;
-      int32_t total = (int32_t)((uint32_t)rmax + (uint32_t)res);
+      cells_acc += cells + wt.hit_rcells[t];
+      int32_t total = (int32_t)((uint32_t)wt.hit_rmax[t] + (uint32_t)res);
       if (sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
         uint32_t at = atomicAdd(&a.tot->cand, 1u);
         if (at < a.cand_cap)
           a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
                             wt.hit_q[t], wt.hit_call[t]};
       }
-      have = false;
     }
+    have = false;
   }
 }
 
-// Fills the first eight cells of both extensions of every hit of the warp's
-// tile.
-template <int TW>
-__device__ __forceinline__ void prepare_first(const GateArgs &a, WarpTile<TW> &wt, uint32_t nt, uint32_t lane) {
+// Fills the first eight cells and the carried word of every hit of the
+// warp's tile for one pass.
+template <int TW, bool LEFT>
+__device__ __forceinline__ void prepare_pass(const GateArgs &a, WarpTile<TW> &wt, uint32_t nt, uint32_t lane) {
   for (uint32_t i = lane; i < nt; i += 32) {
-    const uint32_t r0 = wt.hit_r[i];
-    uint32_t ra, rb, qa, qb;
-    first_group(a.w.ref, r0, &ra, &rb);
-    first_group(a.w.qbuf, wt.hit_q[i], &qa, &qb);
-    wt.u.pass.right[i] = make_uint4(ra, rb, qa, qb);
-    first_group(a.w.ref_rev, a.w.rlen - r0, &ra, &rb);
-    first_group(a.w.qbuf, wt.hit_ql[i], &qa, &qb);
-    wt.u.pass.left[i] = make_uint4(ra, rb, qa, qb);
+    if (LEFT && wt.hit_rmax[i] == kSpilled) continue;
+    uint32_t ra, rb, rc, qa, qb, qc;
+    first_group<LEFT>(a.w.ref, wt.hit_r[i], &ra, &rb, &rc);
+    first_group<LEFT>(a.w.qbuf, wt.hit_q[i], &qa, &qb, &qc);
+    wt.u.pass.first[i] = make_uint4(ra, rb, qa, qb);
+    wt.u.pass.carry[i] = make_uint2(rc, qc);
   }
 }
 
@@ -345,7 +368,7 @@ __global__ void __launch_bounds__(kGateThreads) gate_kernel(GateArgs a) {
     const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
     const uint32_t e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
     uint32_t c = a.tile_call[j];  // calls only advance with the position
-    __syncwarp();                 // the previous tile's gate is done with the union
+    __syncwarp();                 // the previous tile's left pass is done with the union
     for (uint32_t i = lane; i < nt; i += 32) wt.u.setup.hit_slot[i] = 0;
     __syncwarp();
     // (1) slots overlapping the tile
@@ -394,15 +417,18 @@ __global__ void __launch_bounds__(kGateThreads) gate_kernel(GateArgs a) {
       uint32_t nl = min(r0, q0 - cd.qoff);
       wt.hit_r[i] = r0;
       wt.hit_q[i] = q0;
-      wt.hit_ql[i] = cd.qoff_rev + cd.qlen - (q0 - cd.qoff);
       wt.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
       wt.hit_call[i] = hc;
     }
     __syncwarp();
-    // (3) the score gate, both extensions of a hit by one lane
-    prepare_first<TW>(a, wt, nt, lane);
+    // (3) the score gate: right pass, then left pass
+    prepare_pass<TW, false>(a, wt, nt, lane);
     __syncwarp();
-    gate_run<TW>(a, subb, wt, nt, h0, cells_acc);
+    gate_phase<TW, false>(a, subb, wt, nt, h0, cells_acc);
+    __syncwarp();
+    prepare_pass<TW, true>(a, wt, nt, lane);
+    __syncwarp();
+    gate_phase<TW, true>(a, subb, wt, nt, h0, cells_acc);
   }
   for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
   if (lane == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);

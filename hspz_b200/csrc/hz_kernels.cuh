@@ -39,12 +39,6 @@ __global__ void encode_kernel(const uint8_t *__restrict__ ascii, uint64_t n, uin
   }
 }
 
-// dst[i] = src[n - 1 - i]: the reversed copy of a code block.
-__global__ void reverse_kernel(const uint8_t *__restrict__ src, uint64_t n, uint8_t *__restrict__ dst) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[n - 1 - i];
-}
-
 // ---------------------------------------------------------------------------
 // Spaced-seed hash on device codes: INVALID unless every base of the window
 // is uppercase ACGT (code < 4); else the care digits, first care position

@@ -27,13 +27,11 @@ struct CallDev {
   uint32_t qlen;     // block length (right edge of the extension)
   uint32_t start;    // first seed position of the call (block coordinates)
   uint32_t pos_off;  // first flat position of the call in the wave
-  uint32_t qoff_rev;  // offset of the same strand block reversed
 };
 
 // Inputs shared by the lookup, scope and gate kernels.
 struct WaveIn {
-  const uint8_t *ref;      // reference codes (padded on both sides)
-  const uint8_t *ref_rev;  // the same reversed (padded)
+  const uint8_t *ref;  // reference codes (padded on both sides)
   uint32_t rlen;
   const uint8_t *qbuf;  // query store (padded)
   const uint32_t *index_table;
