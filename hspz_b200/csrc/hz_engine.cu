@@ -261,6 +261,10 @@ struct hz_engine {
   uint64_t index_len = 0;
   DBuf<uint32_t> pos_table;
   uint64_t n_pos = 0;
+  // per k-mer: hits of its exact seed and all its transition seeds, capped
+  // per seed (the hit count of a query position with that k-mer)
+  DBuf<uint32_t> nbr_hits;
+  bool has_nbr = false;
   bool has_target = false;
   bool owns_target = true;         // false for serving workers that share the owner's tables
   struct Server *server = nullptr;  // the serving loop, while one runs
@@ -573,6 +577,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
   w.shape = e->shape;
   w.per_pos = seeds ? 1u : e->per_pos(transitions);
   w.occ_cap = e->cfg.occ_cap;
+  w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
 
   for (int attempt = 0; attempt < 4; attempt++) {
     uint32_t scope_cap = std::max<uint32_t>(e->scope_cap, (uint32_t)n * 2 + 16);
@@ -737,6 +742,24 @@ void query_calls(const hz_engine *e, uint32_t qid, std::vector<HostCall> *out) {
         out->push_back(HostCall{qid, iv, rev, (uint32_t)c, (uint32_t)std::min<uint64_t>(c + e->cfg.wga_chunk, (uint64_t)b + 1)});
     }
   }
+}
+
+// The per-k-mer neighbourhood hit counts, for seed patterns of at most 14
+// care positions (a 4^k table of at most 1 GB); larger patterns look up
+// every seed of a position instead.
+int build_nbr_hits(hz_engine *e, uint64_t index_len) {
+  e->has_nbr = false;
+  if (e->shape.kmer_size > 14) return HZ_OK;
+  cudaStream_t s = e->st;
+  TRY(e->nbr_hits.ensure(index_len, s));
+  const uint32_t *idx = e->index_table.p;
+  uint32_t *out = e->nbr_hits.p;
+  const uint32_t ks = e->shape.kmer_size, cap = e->cfg.occ_cap;
+  TRY(e->launch("nbr_hits", [&] {
+    nbr_hits_kernel<<<grid_for(index_len, 256), 256, 0, s>>>(idx, index_len, ks, cap, out);
+  }));
+  e->has_nbr = true;
+  return HZ_OK;
 }
 
 // Replaces the query store with `nq` ASCII blocks; each is encoded forward
@@ -913,6 +936,7 @@ void hz_engine_destroy(hz_engine *e) {
     e->ref.buf.release();
     e->index_table.release();
     e->pos_table.release();
+    e->nbr_hits.release();
   }
   e->qstore.buf.release();
   e->qascii.release();
@@ -987,6 +1011,7 @@ int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t in
   if (pos_len) CK(cudaMemcpyAsync(e->pos_table.p, pos_table, pos_len * 4, cudaMemcpyHostToDevice, s));
   if (ref_len) CK(cudaMemcpyAsync(e->ref.base(), ref_seq, ref_len, cudaMemcpyHostToDevice, s));
   TRY(e->sync());
+  TRY(build_nbr_hits(e, index_len));
   e->index_len = index_len;
   e->n_pos = pos_len;
   e->rlen = (uint32_t)ref_len;
@@ -1101,6 +1126,7 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   total.release();
   hist.release();
   hpartial.release();
+  TRY(build_nbr_hits(e, index_len));
   e->index_len = index_len;
   e->n_pos = n_valid;
   e->rlen = (uint32_t)len;
@@ -1213,6 +1239,7 @@ int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint
     w.shape = e->shape;
     w.per_pos = e->per_pos(transitions);
     w.occ_cap = e->cfg.occ_cap;
+  w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
     TRY(e->launch("lookup_count", [&] {
       lookup_count_kernel<<<(w.npos + kCountPerBlock - 1) / kCountPerBlock, kCountThreads, 0, e->st>>>(w, e->pos_hits.p,
                                                                                                        e->tot.p);
@@ -1718,6 +1745,9 @@ int clone_shared(hz_engine *e, hz_engine **out) {
   w->index_len = e->index_len;
   w->pos_table.p = e->pos_table.p;
   w->pos_table.cap = e->pos_table.cap;
+  w->nbr_hits.p = e->nbr_hits.p;
+  w->nbr_hits.cap = e->nbr_hits.cap;
+  w->has_nbr = e->has_nbr;
   w->n_pos = e->n_pos;
   w->has_target = true;
   w->owns_target = false;

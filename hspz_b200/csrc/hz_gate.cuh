@@ -338,7 +338,7 @@ __device__ __forceinline__ void prepare_pass(const GateArgs &a, WarpTile<TW> &wt
 
 // Bucket lookups issued per group of seeds, so their loads are in flight
 // together.
-constexpr uint32_t kLookupBatch = 4;
+constexpr uint32_t kLookupBatch = 8;
 
 template <int TW>
 __global__ void __launch_bounds__(kGateThreads) gate_kernel(GateArgs a) {

@@ -44,10 +44,22 @@ __global__ void encode_kernel(const uint8_t *__restrict__ ascii, uint64_t n, uin
 // is uppercase ACGT (code < 4); else the care digits, first care position
 // most significant.  src/seed.rs:88-101.
 
+// The window is checked a 4-byte word at a time; the aligned words may
+// reach up to three bytes before and after it, which every code buffer's
+// padding covers.
 __device__ __forceinline__ uint32_t kmer_at(const uint8_t *__restrict__ codes, uint64_t pos,
                                             const ShapeDev &sh) {
+  const uint8_t *p = codes + pos;
+  const uint32_t off = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3u);
+  const uint32_t *wp = reinterpret_cast<const uint32_t *>(p - off);
+  const uint32_t nbytes = off + sh.size;  // bytes from the first aligned word to the window's end
   uint32_t bad = 0;
-  for (uint32_t i = 0; i < sh.size; i++) bad |= codes[pos + i] & 0xFCu;
+  for (uint32_t b = 0; b < nbytes; b += 4) {
+    uint32_t x = __ldg(wp + (b >> 2)) & 0xFCFCFCFCu;
+    if (b == 0) x &= 0xFFFFFFFFu << (8u * off);                       // bytes before the window
+    if (b + 4 > nbytes) x &= 0xFFFFFFFFu >> (8u * (b + 4 - nbytes));  // bytes after it
+    bad |= x;
+  }
   if (bad) return kInvalidKmer;
   uint32_t kmer = 0;
   for (uint32_t t = 0; t < sh.kmer_size; t++) kmer = (kmer << 2) + codes[pos + sh.pos[t]];

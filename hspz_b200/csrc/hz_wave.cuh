@@ -43,6 +43,7 @@ struct WaveIn {
   ShapeDev shape;
   uint32_t per_pos;  // seeds per position: 1 + kmer_size with transitions, else 1
   uint32_t occ_cap;
+  const uint32_t *nbr_hits;  // per k-mer hits of all 1 + kmer_size seeds, or null
 };
 
 // Device-side counters of a wave.
@@ -109,6 +110,35 @@ __device__ __forceinline__ uint32_t bucket(const WaveIn &w, uint32_t k, uint32_t
   return c;
 }
 
+// Per k-mer: the capped hit counts of its exact seed and of its kmer_size
+// transition seeds, summed -- what lookup_count adds up for a query
+// position with that k-mer (u32, wrapping like that sum).
+__global__ void nbr_hits_kernel(const uint32_t *__restrict__ index_table, uint64_t n, uint32_t kmer_size,
+                                uint32_t occ_cap, uint32_t *__restrict__ out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t kmer = (uint32_t)i;
+    uint32_t hi[kMaxCare + 1], lo[kMaxCare + 1];
+#pragma unroll
+    for (uint32_t v = 0; v < kMaxCare + 1; v++) {
+      hi[v] = lo[v] = 0;
+      if (v <= kmer_size) {
+        const uint32_t k = seed_variant(kmer, v);
+        hi[v] = __ldg(index_table + k);
+        lo[v] = k ? __ldg(index_table + k - 1) : 0u;
+      }
+    }
+    uint32_t sum = 0;
+#pragma unroll
+    for (uint32_t v = 0; v < kMaxCare + 1; v++) {
+      uint32_t c = hi[v] - lo[v];
+      if (occ_cap && c > occ_cap) c = 0;
+      sum += c;
+    }
+    out[i] = sum;
+  }
+}
+
 // last index in [lo, hi) whose value is <= h (caller guarantees one exists)
 __device__ __forceinline__ uint32_t last_le(const unsigned long long *v, uint32_t lo, uint32_t hi,
                                             unsigned long long h) {
@@ -140,11 +170,28 @@ __global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, u
     while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
     CallDev cd = w.calls[c];
     uint32_t qpos, kmer, sum = 0;
-    if (position_seed(w, cd, p, &qpos, &kmer)) {
+    if (position_seed(w, cd, p, &qpos, &kmer) && w.nbr_hits && w.per_pos > 1) {
       valid++;
-      for (uint32_t v = 0; v < w.per_pos; v++) {
-        uint32_t beg;
-        sum += bucket(w, seed_variant(kmer, v), &beg);
+      sum = __ldg(w.nbr_hits + kmer);
+    } else if (kmer != kInvalidKmer) {
+      valid++;
+      // every seed's bucket bounds are loaded before any is used, so the
+      // loads are in flight together
+      uint32_t hi[kMaxCare + 1], lo[kMaxCare + 1];
+#pragma unroll
+      for (uint32_t v = 0; v < kMaxCare + 1; v++) {
+        hi[v] = lo[v] = 0;
+        if (v < w.per_pos) {
+          const uint32_t k = seed_variant(kmer, v);
+          hi[v] = __ldg(w.index_table + k);
+          lo[v] = k ? __ldg(w.index_table + k - 1) : 0u;
+        }
+      }
+#pragma unroll
+      for (uint32_t v = 0; v < kMaxCare + 1; v++) {
+        uint32_t c = hi[v] - lo[v];
+        if (w.occ_cap && c > w.occ_cap) c = 0;  // find_num_hits with the occurrence cap
+        sum += c;
       }
     }
     pos_hits[p] = sum;
