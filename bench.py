@@ -381,12 +381,23 @@ def run_ours(args, rank, world, local_rank):
             qarr[i].ascii = t.data_ptr() if t.numel() else None
             qarr[i].len = t.numel()
 
+        parts = {"load_target": 0.0, "stage_queries": 0.0, "run_batched": 0.0}
+
         def e2e_step():
+            # each call returns once its work is done, so the host clock
+            # splits the step into its parts
             hits = d2h = 0
             for pb in pin_b:  # per reference bin: Engine::new + swap_query (src/run.rs:816-887)
+                t0 = time.perf_counter()
                 N.check(L.hz_engine_load_target(e2._h, C.c_void_p(pb.data_ptr()), pb.numel()))
+                t1 = time.perf_counter()
                 N.check(L.hz_stage_queries(e2._h, qarr, len(pin_q)))
+                t2 = time.perf_counter()
                 recs, st = e2.run_batched()
+                t3 = time.perf_counter()
+                parts["load_target"] += t1 - t0
+                parts["stage_queries"] += t2 - t1
+                parts["run_batched"] += t3 - t2
                 hits += st["hits"]
                 d2h += recs.nbytes
             return hits, d2h
@@ -394,6 +405,8 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(max(1, args.warmup)):
             e2e_step()
         barrier()
+        for k in parts:
+            parts[k] = 0.0
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         res = [e2e_step() for _ in range(args.steps)]
@@ -402,7 +415,8 @@ def run_ours(args, rank, world, local_rank):
         ems = max_over_ranks(t0.elapsed_time(t1))
         e2e = {"value": res[-1][0] * args.steps * world / (ems / 1000), "unit": UNIT,
                "h2d_bytes_per_step": int(sum(p.numel() for p in pin_b) + len(pin_b) * sum(p.numel() for p in pin_q)),
-               "d2h_bytes_per_step": int(res[-1][1]), "ms_per_step": ems / args.steps, "form": "batched"}
+               "d2h_bytes_per_step": int(res[-1][1]), "ms_per_step": ems / args.steps, "form": "batched",
+               "host_ms_per_step": {k: round(v * 1000 / args.steps, 2) for k, v in parts.items()}}
         e2.close()
 
     cpu = None

@@ -278,7 +278,7 @@ struct hz_engine {
   // wave buffers
   DBuf<CallDev> calls;
   DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope, tile_first, tile_call;
-  uint32_t tile_cap = 1u << 22;  // entries of the gate's tile table (grows when a wave needs more)
+  uint32_t tile_cap = 1u << 23;  // entries of the gate's tile table (grows when a wave needs more)
   DBuf<unsigned long long> np_excl, call_hit_lo, scope_lo;
   DBuf<HitNz> np_partial, np_grand;
   DBuf<WaveTotals> tot;
