@@ -60,6 +60,7 @@ int fail(int code, const char *fmt, ...) {
   } while (0)
 
 constexpr size_t kPad = 64;  // bytes of padding before and after every sequence buffer
+constexpr uint64_t kKeepBuildScratch = 2ull << 30;  // seed table build memory kept for the next build
 
 // Grow-only device buffer.  Growing waits for the stream, because a queued
 // kernel may still read the old allocation.
@@ -265,6 +266,23 @@ struct hz_engine {
   // per seed (the hit count of a query position with that k-mer)
   DBuf<uint32_t> nbr_hits;
   bool has_nbr = false;
+  // working memory of the on-device seed table build, kept between builds
+  // of up to kKeepBuildScratch bytes (per-bin loads reuse it)
+  struct BuildScratch {
+    DBuf<uint8_t> ascii, junk;
+    DBuf<uint32_t> kmers, flags, keys, vals, keys2, vals2, partial, total, hist, hpartial, excl, ipart;
+    uint64_t bytes() const {
+      return ascii.cap + junk.cap +
+             4 * (kmers.cap + flags.cap + keys.cap + vals.cap + keys2.cap + vals2.cap + partial.cap + total.cap +
+                  hist.cap + hpartial.cap + excl.cap + ipart.cap);
+    }
+    void release() {
+      ascii.release();
+      junk.release();
+      for (auto *b : {&kmers, &flags, &keys, &vals, &keys2, &vals2, &partial, &total, &hist, &hpartial, &excl, &ipart})
+        b->release();
+    }
+  } build;
   bool has_target = false;
   bool owns_target = true;         // false for serving workers that share the owner's tables
   struct Server *server = nullptr;  // the serving loop, while one runs
@@ -940,6 +958,7 @@ void hz_engine_destroy(hz_engine *e) {
   }
   e->qstore.buf.release();
   e->qascii.release();
+  e->build.release();
   for (auto &s : e->slot) s.seeds.release();
   e->calls.release();
   e->pos_hits.release();
@@ -1033,7 +1052,8 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   uint64_t num_steps = (len + offset) > sh.size ? (len + offset - sh.size) / step : 0;
 
   // ASCII -> device codes
-  DBuf<uint8_t> ascii, junk;
+  auto &bs = e->build;
+  DBuf<uint8_t> &ascii = bs.ascii, &junk = bs.junk;
   TRY(ascii.ensure(len + 1, st));
   TRY(e->ref.ensure(len, st));
   TRY(junk.ensure(len + 1, st));
@@ -1046,7 +1066,9 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   TRY(e->index_table.ensure(index_len, st));
   CK(cudaMemsetAsync(e->index_table.p, 0, index_len * 4, st));
 
-  DBuf<uint32_t> kmers, flags, keys, vals, keys2, vals2, partial, total, hist, hpartial;
+  DBuf<uint32_t> &kmers = bs.kmers, &flags = bs.flags, &keys = bs.keys, &vals = bs.vals, &keys2 = bs.keys2,
+                 &vals2 = bs.vals2, &partial = bs.partial, &total = bs.total, &hist = bs.hist,
+                 &hpartial = bs.hpartial;
   uint64_t n_valid = 0;
   if (num_steps) {
     TRY(kmers.ensure(num_steps, st));
@@ -1099,7 +1121,7 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
   TRY(e->pos_table.ensure(1, st));
   // index_table = inclusive cumulative bucket counts (src/seed.rs:162-164)
   {
-    DBuf<uint32_t> excl, ipart;
+    DBuf<uint32_t> &excl = bs.excl, &ipart = bs.ipart;
     TRY(excl.ensure(index_len, st));
     TRY(ipart.ensure(scan_tiles(index_len) + 1, st));
     TRY(total.ensure(1, st));
@@ -1111,21 +1133,8 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
     }));
     CK(cudaMemcpyAsync(e->index_table.p, excl.p, index_len * 4, cudaMemcpyDeviceToDevice, st));
     TRY(e->sync());
-    excl.release();
-    ipart.release();
   }
-  ascii.release();
-  junk.release();
-  kmers.release();
-  flags.release();
-  keys.release();
-  vals.release();
-  keys2.release();
-  vals2.release();
-  partial.release();
-  total.release();
-  hist.release();
-  hpartial.release();
+  if (bs.bytes() > kKeepBuildScratch) bs.release();
   TRY(build_nbr_hits(e, index_len));
   e->index_len = index_len;
   e->n_pos = n_valid;
