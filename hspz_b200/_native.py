@@ -98,6 +98,8 @@ SIGNATURES = {
     "hz_seed_and_filter": (C.c_int, [P, U32, C.c_int, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_run_pass": (C.c_int, [P, C.POINTER(P), PU64, C.POINTER(StatsC)]),
     "hz_dedup_and_order": (C.c_int, [P, U64, PU64]),
+    "hz_render_records": (C.c_int, [P, U64, C.POINTER(C.c_char_p), U32, C.POINTER(C.c_char_p), U32, C.c_char,
+                                    C.POINTER(P), PU64]),
     "hz_dedup_and_order_device_noalloc": (C.c_int, [P, U32, P, P, P]),
     "hz_stage_queries": (C.c_int, [P, C.POINTER(QueryC), U32]),
     "hz_select_query": (C.c_int, [P, U32]),

@@ -1523,6 +1523,66 @@ int hz_dedup_and_order_device_noalloc(const hz_segment_pair *d_in, uint32_t n, h
   return HZ_OK;
 }
 
+int hz_render_records(const hz_segment_record *recs, uint64_t n, const char *const *r_names, uint32_t nr,
+                      const char *const *q_names, uint32_t nq, char strand, char **out, uint64_t *out_len) {
+  if (!out || !out_len || (n && (!recs || !r_names || !q_names))) return fail(HZ_E_INVALID, "null argument");
+  *out = nullptr;
+  *out_len = 0;
+  std::vector<size_t> rl(nr), ql(nq);
+  for (uint32_t i = 0; i < nr; i++) rl[i] = r_names[i] ? strlen(r_names[i]) : 0;
+  for (uint32_t i = 0; i < nq; i++) ql[i] = q_names[i] ? strlen(q_names[i]) : 0;
+  // exact size first: names + up to 20 digits per number + separators
+  uint64_t cap = 1;
+  for (uint64_t i = 0; i < n; i++) {
+    if (recs[i].r_chr >= nr || recs[i].q_chr >= nq)
+      return fail(HZ_E_INVALID, "record %llu names chromosome (%u, %u) outside the tables (%u, %u)",
+                  (unsigned long long)i, recs[i].r_chr, recs[i].q_chr, nr, nq);
+    cap += rl[recs[i].r_chr] + ql[recs[i].q_chr] + 5 * 20 + 11 + 8;
+  }
+  char *buf = (char *)malloc(cap);
+  if (!buf) return fail(HZ_E_OOM, "host allocation of %llu bytes", (unsigned long long)cap);
+  char *w = buf;
+  auto num = [&](unsigned long long v) {
+    char tmp[24];
+    int k = 0;
+    do {
+      tmp[k++] = (char)('0' + v % 10);
+      v /= 10;
+    } while (v);
+    while (k) *w++ = tmp[--k];
+  };
+  for (uint64_t i = 0; i < n; i++) {
+    const hz_segment_record &r = recs[i];
+    memcpy(w, r_names[r.r_chr], rl[r.r_chr]);
+    w += rl[r.r_chr];
+    *w++ = '\t';
+    num(r.r_start);
+    *w++ = '\t';
+    num(r.r_end);
+    *w++ = '\t';
+    memcpy(w, q_names[r.q_chr], ql[r.q_chr]);
+    w += ql[r.q_chr];
+    *w++ = '\t';
+    num(r.q_start);
+    *w++ = '\t';
+    num(r.q_end);
+    *w++ = '\t';
+    *w++ = strand;
+    *w++ = '\t';
+    if (r.score < 0) {
+      *w++ = '-';
+      num((unsigned long long)(-(long long)r.score));
+    } else {
+      num((unsigned long long)r.score);
+    }
+    *w++ = '\n';
+  }
+  *w = 0;
+  *out = buf;
+  *out_len = (uint64_t)(w - buf);
+  return HZ_OK;
+}
+
 int hz_dedup_and_order(hz_segment_pair *h, uint64_t n, uint64_t *n_out) {
   if ((n && !h) || !n_out) return fail(HZ_E_INVALID, "null argument");
   *n_out = dedup_and_order(h, n);

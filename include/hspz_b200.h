@@ -161,6 +161,28 @@ int hz_select_query(hz_engine *e, uint32_t index);
  * hz_run_pass returns for that query alone. */
 int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *stats);
 
+/* One line of a .segments file (hsp::Record, src/hsp.rs:179-187): the
+ * chromosome indices into the reference and query tables and the 1-based,
+ * chromosome-relative coordinates (end = start + length). */
+typedef struct hz_segment_record {
+  uint32_t r_chr;
+  uint32_t q_chr;
+  uint64_t r_start;
+  uint64_t r_end;
+  uint64_t q_start;
+  uint64_t q_end;
+  int32_t score;
+  uint32_t pad;
+} hz_segment_record;
+
+/* render_records (src/hsp.rs:234-252): the text of a .segments file, one
+ * tab-separated line per record -- reference name, start, end, query name,
+ * start, end, strand ('+' or '-'), score.  Names are NUL-terminated; *out is
+ * NUL-terminated, *out_len excludes the NUL, freed with hz_free.  A host-only
+ * entry point (no device needed). */
+int hz_render_records(const hz_segment_record *recs, uint64_t n, const char *const *r_names, uint32_t nr,
+                      const char *const *q_names, uint32_t nq, char strand, char **out, uint64_t *out_len);
+
 /* dedup_and_order (src/hsp.rs:94-126) on host records, in place; returns
  * the kept count in *n_out. */
 int hz_dedup_and_order(hz_segment_pair *h, uint64_t n, uint64_t *n_out);
