@@ -9,7 +9,8 @@ one transition, HOXD70, X-drop 910, HSP threshold 3000, both strands.
 --config 3: a resident 200 Mbp target against 512 query chunks with
 log-uniform lengths in 10 kbp-2 Mbp carrying planted homology at 5-35%.
 
---config 4: repeat-dense 1 Gbp target (10 bins) vs 1 Gbp query with a
+--config 1: the reference's CPU-sized case, 1 Mbp x 1 Mbp (the CPU baseline
+covers all of it).  --config 4: repeat-dense 1 Gbp target (10 bins) vs 1 Gbp query with a
 per-seed occurrence cap of 1000.  --config 5: the serving loop over a
 resident 3 Gbp target under a Poisson request stream (p50/p99 latency and
 throughput; see run_serving).
@@ -21,7 +22,7 @@ batched form (all calls of a bin in shared waves: one lookup, one persistent
 gate launch over a device work queue, one read-back per wave).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config 2|3|4|5] [--form both|batched|plain] [--scale S]
+                  [--config 1|2|3|4|5] [--form both|batched|plain] [--scale S]
 
 One JSON line on rank 0.  `value` is seed hits/s over all ranks for the
 batched form with targets and queries resident in HBM; `e2e` is the same
@@ -59,6 +60,9 @@ def peaks():
 def workload(config: int, scale: float):
     """(target bins, query blocks) as ASCII arrays."""
     from hspz_b200 import synth
+    if config == 1:
+        t, q = synth.config1(seed=1, scale=scale)
+        return [t], [q]
     if config == 3:
         target, chunks = synth.config3(seed=3, scale=scale)
         return [target], chunks
@@ -75,6 +79,7 @@ def occ_cap(config: int) -> int:
 
 
 WORKLOADS = {
+    1: "config1: 1 Mbp target vs 1 Mbp query, 200 planted segments at 15%",
     2: "config2: 100 Mbp target as 10 bins x 10 Mbp vs 100 Mbp query",
     3: "config3: 200 Mbp resident target vs 512 query chunks (log-uniform 10 kbp-2 Mbp)",
     4: "config4: repeat-dense 1 Gbp target as 10 bins vs 1 Gbp query (45% from 500 repeat families, "
@@ -183,8 +188,10 @@ def cpu_sample(bins, queries, threads: int, budget_batches: int, cap: int = 0):
 
 
 def cpu_sample_text(args, st, dt):
+    if args.config == 1:
+        return f"the whole pass ({st['calls']} seed_and_filter calls, {st['hits']} hits, {dt:.1f} s)"
     return (f"bin 0 x the first {args.cpu_batches} seed_and_filter calls of the "
-            f"{'query' if args.config == 2 else 'longest query chunk'} ({st['hits']} hits, {dt:.1f} s)")
+            f"{'query' if args.config in (2, 4) else 'longest query chunk'} ({st['hits']} hits, {dt:.1f} s)")
 
 
 def run_reference(args, rank):
@@ -598,7 +605,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--form", default="both", choices=["both", "batched", "plain"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-batches", type=int, default=80)
