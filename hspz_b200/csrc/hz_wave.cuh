@@ -514,6 +514,102 @@ __device__ __forceinline__ void exact_dir(const uint8_t *ref, const uint8_t *qry
   }
 }
 
+// The same direction with four consecutive cells per lane, 128 cells per
+// warp step: the lane sums its four cells, the warp scans the lane totals and
+// the lanes' largest sums, and the first dropping cell, the maximum before it
+// and that maximum's earliest position follow exactly as above.  Long
+// extensions (the occurrence-capped repeat tails and homologous runs that
+// reach the gate's cap) need a quarter of the scan steps.
+template <bool LEFT>
+__device__ __forceinline__ void exact_dir4(const uint8_t *ref, const uint8_t *qry, const int32_t *sub, int32_t X,
+                                           uint32_t r0, uint32_t q0, uint32_t nmax, uint32_t lane, int32_t *out_max,
+                                           int32_t *out_pos, unsigned long long *cells) {
+  int32_t prev_s = 0, prev_m = 0, prev_pos = LEFT ? 0 : -1;
+  for (uint32_t tile = 0;; tile += 128) {
+    const uint32_t k0 = tile + 4u * lane;
+    int32_t p[4];
+    int32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t k = k0 + (uint32_t)i;
+      int32_t sc = 0;
+      if (k < nmax) {
+        uint32_t rc = LEFT ? ref[r0 - 1 - k] : ref[r0 + k];
+        uint32_t qc = LEFT ? qry[q0 - 1 - k] : qry[q0 + k];
+        sc = sub[rc * kNuc + qc];
+      }
+      acc = (int32_t)((uint32_t)acc + (uint32_t)sc);
+      p[i] = acc;
+    }
+    const int32_t incl = warp_incl_sum(acc, lane);
+    const int32_t base = (int32_t)((uint32_t)prev_s + (uint32_t)incl - (uint32_t)acc);
+    int32_t ts[4], lm[4];  // running sums of the lane's cells; the lane's running maximum of them
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      ts[i] = (int32_t)((uint32_t)base + (uint32_t)p[i]);
+      lm[i] = i ? max(lm[i - 1], ts[i]) : ts[i];
+    }
+    // the running maximum before the lane's first cell: prev_m and every
+    // earlier lane's cells
+    const int32_t upto = warp_incl_max(max(lm[3], prev_m));
+    int32_t before = __shfl_up_sync(0xffffffffu, upto, 1);
+    if (lane == 0) before = prev_m;
+    int32_t Mi[4];
+    uint32_t dbits = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      Mi[i] = max(before, lm[i]);
+      dbits |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)ts[i]) > X) << i;
+    }
+    const uint32_t dl = __ballot_sync(0xffffffffu, dbits != 0);
+    uint32_t first = 128;
+    if (dl) {
+      const uint32_t fl = (uint32_t)(__ffs(dl) - 1);
+      const uint32_t fi = (uint32_t)(__ffs(__shfl_sync(0xffffffffu, dbits, fl)) - 1);
+      first = 4u * fl + fi;
+    }
+    // the maximum before the first dropping cell (or over the whole step)
+    int32_t mx;
+    if (first == 0) {
+      mx = prev_m;
+    } else {
+      const uint32_t c = first - 1, src = c >> 2, idx = c & 3u;
+      int32_t mine = Mi[0];
+#pragma unroll
+      for (int i = 1; i < 4; i++)
+        if ((uint32_t)i == idx) mine = Mi[i];
+      mx = __shfl_sync(0xffffffffu, mine, src);
+    }
+    int32_t pos;
+    if (mx == prev_m) {
+      pos = prev_pos;
+    } else {
+      uint32_t wbits = 0;
+#pragma unroll
+      for (int i = 0; i < 4; i++) wbits |= (uint32_t)(ts[i] == mx && 4u * lane + (uint32_t)i < first) << i;
+      const uint32_t wl = __ballot_sync(0xffffffffu, wbits != 0);
+      const uint32_t l = (uint32_t)(__ffs(wl) - 1);
+      const uint32_t wi = (uint32_t)(__ffs(__shfl_sync(0xffffffffu, wbits, l)) - 1);
+      pos = (int32_t)(4u * l + wi + tile) + (LEFT ? 1 : 0);
+    }
+    if (dl) {
+      *cells += min(tile + first + 1, nmax);
+      *out_max = mx;
+      *out_pos = pos;
+      return;
+    }
+    if (tile + 128 >= nmax) {  // the step reached the edge
+      *cells += nmax;
+      *out_max = mx;
+      *out_pos = pos;
+      return;
+    }
+    prev_s = __shfl_sync(0xffffffffu, ts[3], 31);
+    prev_m = mx;
+    prev_pos = pos;
+  }
+}
+
 constexpr int kExactThreads = 128;
 
 __global__ void __launch_bounds__(kExactThreads) exact_kernel(ExactArgs a) {
@@ -532,8 +628,15 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(ExactArgs a) {
     uint32_t q0 = cd.q0 - call.qoff, r0 = cd.r0;
     unsigned long long cells = 0;
     int32_t rmax, rpos, lmax, lpos;
-    exact_dir<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos, &cells);
-    exact_dir<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
+    if (is_long) {  // reached the gate's cap: long runs, four cells per lane
+      exact_dir4<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos,
+                        &cells);
+      exact_dir4<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
+    } else {
+      exact_dir<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos,
+                       &cells);
+      exact_dir<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
+    }
     if (is_long) cells_acc += cells;
     int32_t total = (int32_t)((uint32_t)rmax + (uint32_t)lmax);
     int32_t extent = (int32_t)((uint32_t)rpos + (uint32_t)lpos);

@@ -72,3 +72,21 @@ def test_repeat_dense_batched_equals_plain(pair):
             for f in FIELDS:
                 assert np.array_equal(sel[f], want[f]), (i, f)
     assert st["hits"] == hits
+
+
+@pytest.mark.parametrize("gate_cap", [8, 64])
+def test_long_extensions_through_the_warp_kernel(pair, gate_cap):
+    """A small gate cap sends most hits to the warp kernel as long
+    extensions (four cells per lane there); records and counts still equal
+    the oracle's."""
+    t, q = pair
+    sm = EngineConfig().sub_mat
+    want, st_o = oracle_run(t, q, sm, occ_cap=1000)
+    with Engine(EngineConfig(occ_cap=1000)) as e:
+        e.set_tuning(gate_cap=gate_cap)
+        e.load_target(t)
+        e.swap_query_ascii(q)
+        got, st = e.run_pass()
+    assert got.tobytes() == want.tobytes()
+    for k in ("hits", "raw_hsps", "hsps", "cells"):
+        assert st[k] == st_o[k], k
