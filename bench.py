@@ -445,7 +445,8 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "kernel": "gate (fused hit expansion + X-drop score gate)",
                          "achieved": g["achieved"], "peak": peak, "unit": "GB/s",
                          "frac": g["achieved"] / peak if g["achieved"] else None, "traffic": traffic,
-                         "peak_kind": peak_kind,
+                         "peak_kind": peak_kind, "spec_peak": 8000.0,
+                         "frac_of_spec": g["achieved"] / 8000.0 if g["achieved"] else None,
                          "note": "issue-bound integer kernel; algorithmic bytes = 2 B per scored cell + 4 B per hit"},
             "lookup_roofline": dict(head["lookup"], kernel="lookup_count", peak=peak, unit="GB/s",
                                     note="9 B per valid position: code byte, neighbourhood count, count "
