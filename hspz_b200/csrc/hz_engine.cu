@@ -308,6 +308,7 @@ struct hz_engine {
   HBuf<uint32_t> h_raw_scope, h_scope_call;
   // device dedup of the batched form
   bool device_dedup = true;
+  uint32_t device_dedup_min = 1u << 16;  // raw HSPs from which a per-call wave dedups on the device
   DBuf<uint32_t> d_perm_a, d_perm_b, d_keys_a, d_keys_b, d_keep, d_keep_excl, d_hist, d_hpart, d_total;
   DBuf<ScopedHspOut> d_out;
   HBuf<ScopedHspOut> h_out;
@@ -713,7 +714,10 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       st->calls += n;
     }
     if (nraw == 0) return HZ_OK;
-    if (device_dedup) return dedup_on_device(e, nraw, t.n_scopes, out, st);
+    // per-call waves (the plain form) dedup on the host like the reference,
+    // unless the call holds so many raw HSPs that the device sort is faster
+    if (device_dedup || (e->device_dedup && nraw >= e->device_dedup_min))
+      return dedup_on_device(e, nraw, t.n_scopes, out, st);
     TRY(e->h_raw.ensure(nraw));
     TRY(e->h_raw_scope.ensure(nraw));
     TRY(e->h_scope_call.ensure(t.n_scopes + 1));
@@ -1638,6 +1642,9 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
     e->gate_blocks_per_sm = (int)value;
   } else if (k == "device_dedup") {
     e->device_dedup = value != 0;
+  } else if (k == "device_dedup_min") {
+    if (value < 1 || value > 0xFFFFFFFFll) return fail(HZ_E_INVALID, "device_dedup_min must be 1..2^32-1");
+    e->device_dedup_min = (uint32_t)value;
   } else if (k == "graph") {
     e->use_graph = value != 0;
   } else if (k == "wave_positions") {
@@ -1825,6 +1832,7 @@ int clone_shared(hz_engine *e, hz_engine **out) {
   w->gate_blocks_per_sm = e->gate_blocks_per_sm;
   w->wave_positions = e->wave_positions;
   w->device_dedup = e->device_dedup;
+  w->device_dedup_min = e->device_dedup_min;
   w->use_graph = e->use_graph;
   cudaError_t err = cudaStreamCreateWithFlags(&w->own_st, cudaStreamNonBlocking);
   if (err != cudaSuccess) {

@@ -222,7 +222,9 @@ int hz_engine_profile_reset(hz_engine *e);
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
  * "wave_positions" (seed positions per batched wave), "device_dedup" (1: the
- * batched form dedups on the device, 0: on the host as the plain form does),
+ * batched form dedups on the device, and so does a plain-form call holding at
+ * least "device_dedup_min" raw HSPs (default 65536); 0: every dedup on the
+ * host, as the reference does),
  * "graph" (1: the batched form captures each wave's kernel chain as a CUDA
  * graph and replays it, updating the instantiated graph in place). */
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);

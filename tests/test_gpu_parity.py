@@ -208,3 +208,18 @@ def test_tiny_and_empty_inputs():
         e.swap_query_ascii(b"")
         recs, st = e.run_pass()
         assert recs.size == 0
+
+
+def test_plain_form_device_dedup_for_large_calls():
+    """A plain-form call with many raw HSPs dedups on the device; with the
+    threshold at 1 every call does, and the records stay the oracle's."""
+    t, q = synth.config1(seed=4, scale=0.2)
+    sm = EngineConfig().sub_mat
+    want, _ = oracle_run(t, q, sm)
+    with engine_for(sm) as e:
+        e.set_tuning(device_dedup_min=1)
+        e.load_target(t)
+        e.swap_query_ascii(q)
+        got, _ = e.run_pass()
+    assert want.size > 10
+    assert got.tobytes() == want.tobytes()
