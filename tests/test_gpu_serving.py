@@ -160,3 +160,31 @@ def test_failing_request_reports_its_own_error():
         e.serve_stop()
         e.swap_query_ascii(clean)
         assert rows(got) == rows(e.run_pass()[0])
+
+
+def test_many_workers_random_poll_order_and_totals():
+    """Four workers, batches of up to eight, requests polled in random order:
+    every result equals run_pass alone, and the loop's hit total is the sum
+    of the requests' own totals."""
+    rng = np.random.default_rng(11)
+    target, chunks = synth.config3(seed=53, scale=0.01, n_chunks=40)
+    with Engine(EngineConfig()) as ref:
+        ref.load_target(target)
+        want, hits = [], 0
+        for q in chunks:
+            ref.swap_query_ascii(q)
+            r, st = ref.run_pass()
+            want.append(rows(r))
+            hits += st["hits"]
+    with Engine(EngineConfig()) as e:
+        e.load_target(target)
+        e.serve_start(budget_bytes=4 << 30, workers=4, max_batch_queries=8)
+        tickets = [e.serve_submit(q) for q in chunks]
+        order = rng.permutation(len(chunks))
+        for i in order:
+            got, _ = e.serve_poll(tickets[i])
+            assert rows(got) == want[i], i
+        totals, queued, running = e.serve_stats()
+        assert (queued, running) == (0, 0)
+        assert totals["hits"] == hits
+        e.serve_stop()
