@@ -223,3 +223,26 @@ def test_plain_form_device_dedup_for_large_calls():
         got, _ = e.run_pass()
     assert want.size > 10
     assert got.tobytes() == want.tobytes()
+
+
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_files_in_files_out_reproduce_the_frozen_digests(tmp_path, form):
+    """Sequence files -> device seed table -> pass -> .segments files: the
+    frozen smoke digests, with the inputs as FASTA and as gzipped FASTA."""
+    import gzip
+    import shutil
+    from hspz_b200.pipeline import seed_and_filter_files
+    from tests.golden.fixture_pass import FIXTURES
+    for name in sorted(EXPECTED):
+        d = load(name)
+        ref = os.path.join(FIXTURES, f"{name}.ref.fa")
+        qry = tmp_path / f"{name}.qry.fa.gz"
+        with open(os.path.join(FIXTURES, f"{name}.qry.fa"), "rb") as src, gzip.open(qry, "wb") as dst:
+            shutil.copyfileobj(src, dst)
+        out = tmp_path / f"out_{name}_{form}"
+        files = seed_and_filter_files(ref, qry, out_dir=str(out), form=form,
+                                      config=EngineConfig(sub_mat=d["sub_mat"], max_hits=MAX_HITS))
+        n, digest = H.sorted_digest(files)
+        assert (n, len(files), digest) == (EXPECTED[name]["hsps"], EXPECTED[name]["files"],
+                                           EXPECTED[name]["digest"]), name
+        assert sorted(os.listdir(out)) == sorted(files)
