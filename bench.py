@@ -121,7 +121,8 @@ class Clocks:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}_{device}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"hz_clocks_{os.getpid()}_{device}.csv")
 
     def __enter__(self):
         try:
