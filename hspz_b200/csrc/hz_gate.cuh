@@ -141,9 +141,10 @@ __device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint
 }
 
 // Scores one cell whose byte offset into the substitution table is byte SH
-// of T (extracted, zero-extended, by one byte permute); keeps every running sum S and maximum M for the termination path
-// and the group's smallest sum. Since every M_i <= M_7, no cell of the group
-// can have dropped when M_7 - min S <= xdrop.
+// of T (extracted, zero-extended, by one byte permute); keeps every running
+// sum S and maximum M for the termination path and the group's smallest sum.
+// Since every M_i <= M_7, no cell of the group can have dropped when
+// M_7 - min S <= xdrop.
 #define HZ_CELL(T, SH, I)                                                            \
   {                                                                                  \
     int32_t sc = *reinterpret_cast<const int32_t *>(subb + __byte_perm((T), 0u, 0x4440u + (SH) / 8)); \
