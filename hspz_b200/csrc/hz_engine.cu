@@ -1650,6 +1650,10 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   } else if (k == "wave_positions") {
     if (value < 1 || value >= (1ll << 31)) return fail(HZ_E_INVALID, "wave_positions must be 1..2^31-1");
     e->wave_positions = (uint64_t)value;
+  } else if (k == "tile_cap" || k == "cand_cap" || k == "raw_cap") {
+    // starting capacities; a wave that needs more grows them and runs again
+    if (value < 16 || value > 0x7FFFFFFFll) return fail(HZ_E_INVALID, "%s must be 16..2^31-1", key);
+    (k == "tile_cap" ? e->tile_cap : k == "cand_cap" ? e->cand_cap : e->raw_cap) = (uint32_t)value;
   } else {
     return fail(HZ_E_INVALID, "unknown tuning key %s", key);
   }

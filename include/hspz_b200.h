@@ -226,7 +226,10 @@ int hz_engine_profile_reset(hz_engine *e);
  * least "device_dedup_min" raw HSPs (default 65536); 0: every dedup on the
  * host, as the reference does),
  * "graph" (1: the batched form captures each wave's kernel chain as a CUDA
- * graph and replays it, updating the instantiated graph in place). */
+ * graph and replays it, updating the instantiated graph in place),
+ * "tile_cap" / "cand_cap" / "raw_cap" (starting capacities of the gate's
+ * tile table, the candidate list and the raw-HSP list; a wave that needs more
+ * grows them and runs again). */
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
 
 /* Autotuner (no reference counterpart).  Times the batched form on a

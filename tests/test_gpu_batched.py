@@ -127,3 +127,28 @@ def test_graph_replay_profiles_and_autotune_keep_results(workload):
         again, st2 = e.run_batched()
     assert again.tobytes() == base.tobytes()
     assert (st2["hits"], st2["cells"]) == (st0["hits"], st0["cells"])
+
+
+def test_capacity_overflow_reruns_give_the_same_records(workload):
+    """Starting capacities far too small: every wave overflows its tile
+    table, candidate list and raw-HSP list, grows them and runs again; the
+    records and counts are unchanged, in both forms."""
+    target, chunks = workload
+    chunks = chunks[:12]
+    with Engine(EngineConfig()) as e:
+        e.load_target(target)
+        e.stage_queries(chunks)
+        base, st0 = e.run_batched()
+        e.select_query(3)
+        plain0, _ = e.run_pass()
+    with Engine(EngineConfig()) as e:
+        e.set_tuning(tile_cap=16, cand_cap=16, raw_cap=16)
+        e.load_target(target)
+        e.stage_queries(chunks)
+        got, st1 = e.run_batched()
+        e.set_tuning(tile_cap=16, cand_cap=16, raw_cap=16)
+        e.select_query(3)
+        plain1, _ = e.run_pass()
+    assert got.tobytes() == base.tobytes()
+    assert plain1.tobytes() == plain0.tobytes()
+    assert (st1["hits"], st1["cells"], st1["raw_hsps"]) == (st0["hits"], st0["cells"], st0["raw_hsps"])
