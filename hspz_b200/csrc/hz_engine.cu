@@ -598,7 +598,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
   w.occ_cap = e->cfg.occ_cap;
   w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
 
-  for (int attempt = 0; attempt < 4; attempt++) {
+  for (int attempt = 0; attempt < 8; attempt++) {  // each rerun fixes every capacity it found short
     uint32_t scope_cap = std::max<uint32_t>(e->scope_cap, (uint32_t)n * 2 + 16);
     TRY(e->scope_lo.ensure(scope_cap + 1, s));
     TRY(e->scope_call.ensure(scope_cap + 1, s));
