@@ -246,3 +246,19 @@ def test_files_in_files_out_reproduce_the_frozen_digests(tmp_path, form):
         assert (n, len(files), digest) == (EXPECTED[name]["hsps"], EXPECTED[name]["files"],
                                            EXPECTED[name]["digest"]), name
         assert sorted(os.listdir(out)) == sorted(files)
+
+
+@pytest.mark.parametrize("ambiguous", ["n", "iupac", "iupac,5,7"])
+def test_ambiguous_scoring_parity(ambiguous):
+    """--ambiguous scoring (N and IUPAC codes rewarded or penalised) on the
+    fixture with ambiguous bases: the oracle's records."""
+    from hspz_b200.scoring import build_sub_mat
+    d = load("ambiguous")
+    sm = build_sub_mat(ambiguous, 910)
+    want, st_o = oracle_run(d["ref_ascii"], d["qry_ascii"], sm, max_hits=MAX_HITS)
+    with engine_for(sm, max_hits=MAX_HITS) as e:
+        e.load_target(d["ref_ascii"])
+        e.swap_query_ascii(d["qry_ascii"])
+        got, st = e.run_pass()
+    assert got.tobytes() == want.tobytes()
+    assert (st["hits"], st["cells"]) == (st_o["hits"], st_o["cells"])

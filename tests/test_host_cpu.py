@@ -78,3 +78,15 @@ def test_synthetic_inputs_are_seeded():
     assert 0.03 < low < 0.2
     gc = np.mean(np.isin(a1 & 0xDF, np.frombuffer(b"GC", dtype=np.uint8)))
     assert 0.37 < gc < 0.45
+
+
+def test_ambiguous_scoring_variants():  # src/scoring.rs:295-323
+    from hspz_b200.scoring import build_sub_mat
+    nuc = 8
+    m = build_sub_mat("", 910)
+    assert (m[2 * nuc + 2], m[4 * nuc + 4], m[5 * nuc + 5]) == (100, -1000, -1000)
+    assert (m[6 * nuc + 6], m[7 * nuc + 7], m[7]) == (-100, -9100, -9100)
+    m = build_sub_mat("n", 910)
+    assert (m[5 * nuc + 5], m[5], m[6 * nuc + 6]) == (0, 0, -100)
+    m = build_sub_mat("iupac,5,7", 910)
+    assert (m[5 * nuc + 5], m[5], m[6 * nuc + 6]) == (5, -7, 5)
