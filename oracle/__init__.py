@@ -74,6 +74,7 @@ def lib():
         L.hzo_ln_export.restype = C.c_double
         L.hzo_batches.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P]
         L.hzo_batches.restype = C.c_int64
+        L.hzo_chunk_limits.argtypes = [P, C.c_uint64, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
         L.hzo_free.argtypes = [P]
         _lib = L
     return _lib
@@ -171,6 +172,20 @@ def extend_hit(p: Params, ref, qry, r: int, q: int):
 
 def ln(x: float) -> float:
     return lib().hzo_ln_export(x)
+
+
+def chunk_limits(hit_num, max_hits: int):
+    """The MAX_HITS chunk list (start_seed, last_seed, start_hit, end_hit)
+    of one call's inclusive running hit counts; raises ValueError where the
+    reference panics."""
+    h = np.ascontiguousarray(hit_num, dtype=np.uint32)
+    cap = int(h[-1]) // max(max_hits, 1) + 2
+    out = np.zeros(4 * cap, dtype=np.uint32)
+    n = C.c_uint32()
+    rc = lib().hzo_chunk_limits(_ptr(h), h.size, max_hits, _ptr(out), cap, C.byref(n))
+    if rc:
+        raise ValueError(f"chunk_limits failed: {rc}")
+    return [tuple(int(x) for x in out[4 * i: 4 * i + 4]) for i in range(n.value)]
 
 
 def _take(ptr: C.c_void_p, n: int, dtype) -> np.ndarray:

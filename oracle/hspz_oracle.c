@@ -427,6 +427,64 @@ static inline uint32_t hit_count(const hzo_target *t, uint32_t k) {
 
 /* Runs one call on `seeds`.  Output (deduped per MAX_HITS chunk, lastz order,
  * concatenated) is appended to *out.  Returns 0 or a negative code. */
+/* chunk_limits (src/gpu/mod.rs:2394-2420, single-chunk shortcut :1693-1705):
+ * the MAX_HITS split of one call over the inclusive running hit counts
+ * hit_num[0..ns).  Each cut is the last seed whose running count is below the
+ * running limit (partition_point(v < limit) - 1); the next limit is that
+ * count plus max_hits.  A first seed alone above the limit has no valid cut
+ * (the reference panics there): HZO_E_INVALID.  *out is malloc'd. */
+static int chunk_limits(const uint32_t *hit_num, uint64_t ns, uint32_t max_hits, uint32_t (**out)[4],
+                        uint32_t *n_out) {
+  uint32_t num_hits = hit_num[ns - 1];
+  uint32_t(*ch)[4];
+  if (num_hits <= max_hits) {
+    ch = malloc(sizeof(*ch));
+    if (!ch) return HZO_E_OOM;
+    ch[0][0] = 0; ch[0][1] = (uint32_t)(ns - 1); ch[0][2] = 0; ch[0][3] = num_hits;
+    *out = ch;
+    *n_out = 1;
+    return 0;
+  }
+  uint32_t num_iter = num_hits / max_hits + 1;
+  ch = malloc((uint64_t)num_iter * sizeof(*ch));
+  if (!ch) return HZO_E_OOM;
+  uint32_t limit = max_hits, start_seed = 0, start_hit = 0;
+  for (uint32_t it = 0; it + 1 < num_iter; it++) {
+    uint64_t lo = 0, hi = ns;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) / 2;
+      if (hit_num[mid] < limit) lo = mid + 1; else hi = mid;
+    }
+    if (lo == 0) { free(ch); return HZO_E_INVALID; }
+    uint32_t pos = (uint32_t)(lo - 1);
+    ch[it][0] = start_seed; ch[it][1] = pos; ch[it][2] = start_hit; ch[it][3] = hit_num[pos];
+    start_seed = pos + 1;
+    start_hit = hit_num[pos];
+    limit = hit_num[pos] + max_hits;
+  }
+  ch[num_iter - 1][0] = start_seed; ch[num_iter - 1][1] = (uint32_t)(ns - 1);
+  ch[num_iter - 1][2] = start_hit; ch[num_iter - 1][3] = hit_num[ns - 1];
+  *out = ch;
+  *n_out = num_iter;
+  return 0;
+}
+
+/* The chunk list of chunk_limits for tests: up to cap entries of
+ * (start_seed, last_seed, start_hit, end_hit) into out[4 * cap]. */
+int hzo_chunk_limits(const uint32_t *hit_num, uint64_t ns, uint32_t max_hits, uint32_t *out, uint32_t cap,
+                     uint32_t *n_out) {
+  if (ns == 0 || max_hits == 0) return HZO_E_INVALID;
+  uint32_t(*ch)[4];
+  uint32_t n;
+  int rc = chunk_limits(hit_num, ns, max_hits, &ch, &n);
+  if (rc) return rc;
+  for (uint32_t i = 0; i < n && i < cap; i++)
+    for (int k = 0; k < 4; k++) out[4 * i + k] = ch[i][k];
+  *n_out = n;
+  free(ch);
+  return 0;
+}
+
 static int run_call(const hzo_target *t, const uint8_t *qry, uint32_t qlen, const uint64_t *seeds,
                     uint64_t ns, hsp_vec *out, hzo_stats *st) {
   const hzo_params *p = t->p;
@@ -446,37 +504,10 @@ static int run_call(const hzo_target *t, const uint8_t *qry, uint32_t qlen, cons
   if (num_hits == 0) { free(hit_num); return 0; }
 
   /* chunk list: (start_seed, limit_pos, start_hit, end_hit) */
-  uint32_t max_hits = p->max_hits;
   uint32_t nchunks;
   uint32_t(*ch)[4];
-  if (num_hits <= max_hits) {
-    nchunks = 1;
-    ch = malloc(sizeof(*ch));
-    if (!ch) { free(hit_num); return HZO_E_OOM; }
-    ch[0][0] = 0; ch[0][1] = (uint32_t)(ns - 1); ch[0][2] = 0; ch[0][3] = num_hits;
-  } else {
-    uint32_t num_iter = num_hits / max_hits + 1;
-    ch = malloc((uint64_t)num_iter * sizeof(*ch));
-    if (!ch) { free(hit_num); return HZO_E_OOM; }
-    uint32_t limit = max_hits, start_seed = 0, start_hit = 0;
-    for (uint32_t it = 0; it + 1 < num_iter; it++) {
-      /* partition_point(v < limit) - 1 */
-      uint64_t lo = 0, hi = ns;
-      while (lo < hi) {
-        uint64_t mid = (lo + hi) / 2;
-        if (hit_num[mid] < limit) lo = mid + 1; else hi = mid;
-      }
-      if (lo == 0) { free(ch); free(hit_num); return HZO_E_INVALID; } /* reference panics */
-      uint32_t pos = (uint32_t)(lo - 1);
-      ch[it][0] = start_seed; ch[it][1] = pos; ch[it][2] = start_hit; ch[it][3] = hit_num[pos];
-      start_seed = pos + 1;
-      start_hit = hit_num[pos];
-      limit = hit_num[pos] + max_hits;
-    }
-    ch[num_iter - 1][0] = start_seed; ch[num_iter - 1][1] = (uint32_t)(ns - 1);
-    ch[num_iter - 1][2] = start_hit; ch[num_iter - 1][3] = hit_num[ns - 1];
-    nchunks = num_iter;
-  }
+  int crc = chunk_limits(hit_num, ns, p->max_hits, &ch, &nchunks);
+  if (crc) { free(hit_num); return crc; }
 
   hsp_vec raw = {0};
   int rc = 0;

@@ -120,3 +120,23 @@ def test_ln_series_is_close_to_libm():  # src/gpu/kernels.rs:1879-1908
     # series on both sides, not libm accuracy.
     for x in [1.0, 0.5, 0.25, 1e-3, 0.3333333333, 0.999999, 0.7071, 0.70710678118654757]:
         assert abs(oracle.ln(x) - np.log(x)) < 1e-13 * max(1.0, abs(np.log(x)))
+
+
+def test_chunk_limits_walk():  # src/gpu/mod.rs:2644-2668
+    assert oracle.chunk_limits([2, 5, 9], 1000) == [(0, 2, 0, 9)]
+    ch = oracle.chunk_limits([3, 7, 11, 15], 5)
+    assert len(ch) == 4
+    assert ch[0] == (0, 0, 0, 3)  # the first chunk stops before overshooting 5
+    assert all(b[0] == a[1] + 1 for a, b in zip(ch, ch[1:]))  # chunks tile the seed range
+    assert ch[-1][1] == 3
+    with pytest.raises(ValueError):  # a first seed above the limit has no cut
+        oracle.chunk_limits([10, 12], 5)
+
+
+def test_gate_threshold_uses_the_f32_rounded_total():  # src/gpu/kernels.rs:2029-2042
+    import struct
+    f32 = lambda v: struct.unpack("f", struct.pack("f", float(v)))[0]
+    right, left, threshold = 1400, 1600, 3000
+    assert right < threshold and int(f32(right + left)) >= threshold
+    raw, threshold = 16_777_219, 16_777_220  # above 2^24 the f32 conversion can round up
+    assert raw < threshold and int(f32(raw)) >= threshold
