@@ -83,6 +83,14 @@ def test_device_seed_table_is_byte_identical():
             idx_d, pos_d = e.read_tables()
         assert np.array_equal(idx_d, idx_o)
         assert np.array_equal(pos_d, pos_o)
+    # other seed patterns: short, spaced, with explicit transition marks
+    for spec in ("1111", "11011", "1T1T11", "111010010100110111"):
+        idx_o, pos_o = oracle.seed_table(oracle.encode(seq[:50_000].tobytes()), oracle.shape(spec), 1)
+        with engine_for(sm, seed=spec) as e:
+            e.load_target(seq[:50_000])
+            idx_d, pos_d = e.read_tables()
+        assert np.array_equal(idx_d, idx_o), spec
+        assert np.array_equal(pos_d, pos_o), spec
 
 
 def test_config1_full_parity():

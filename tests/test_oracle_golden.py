@@ -140,3 +140,20 @@ def test_gate_threshold_uses_the_f32_rounded_total():  # src/gpu/kernels.rs:2029
     assert right < threshold and int(f32(right + left)) >= threshold
     raw, threshold = 16_777_219, 16_777_220  # above 2^24 the f32 conversion can round up
     assert raw < threshold and int(f32(raw)) >= threshold
+
+
+def test_shapes_and_kmers_restated():  # src/seed.rs:512-538
+    from hspz_b200 import _native as N
+    from hspz_b200 import shape_info
+    assert shape_info("1111") == (4, 4)
+    assert shape_info("11011") == (5, 4)
+    for bad in ("101", "1" * 16):  # care positions must number 4..15
+        with pytest.raises(N.HzError):
+            shape_info(bad)
+    # "1111" packs A C G T as 00 01 10 11; a separator anywhere in the window
+    # (a don't-care position included) kills it; step 1 skips position 0
+    for spec, seq, k, want in (("1111", b"AACGTA&ACGTT", 0b00011011, [1, 7]),
+                               ("11011", b"TACAGT&AC&GT", 0b00011011, [1])):
+        idx, pos = oracle.seed_table(oracle.encode(seq), oracle.shape(spec))
+        lo = int(idx[k - 1]) if k else 0
+        assert pos[lo: int(idx[k])].tolist() == want, spec
