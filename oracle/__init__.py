@@ -9,7 +9,6 @@ from __future__ import annotations
 import ctypes as C
 import os
 import subprocess
-from dataclasses import dataclass
 
 import numpy as np
 

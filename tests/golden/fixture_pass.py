@@ -2,8 +2,6 @@
 set-up of tests/test_oracle_golden.py and the GPU parity tests."""
 import os
 
-import numpy as np
-
 import oracle
 from hspz_b200 import hsp as H
 from hspz_b200 import scoring

@@ -6,7 +6,6 @@ format, in both byte orders and in both versions."""
 import gzip
 import struct
 
-import numpy as np
 import pytest
 
 from hspz_b200 import sequence as S

@@ -1,7 +1,6 @@
 """The batched form against the plain per-chunk form and the oracle: many
 query chunks of uneven length through shared waves must give, per query,
 exactly the records the plain form gives for that query alone."""
-import numpy as np
 import pytest
 
 from hspz_b200 import Engine, EngineConfig

@@ -1,7 +1,5 @@
 """Host-side mirror of the reference's config surface: scoring files
 (src/scoring.rs tests :280-404), sequence helpers and synthetic inputs."""
-import os
-
 import numpy as np
 import pytest
 
