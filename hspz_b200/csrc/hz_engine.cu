@@ -315,7 +315,7 @@ struct hz_engine {
   uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
   // tuning
   int gate_tile = 128;  // hits per gate warp tile
-  uint32_t gate_cap = 256;
+  uint32_t gate_cap = 128;  // the autotuner's usual choice
   int gate_blocks_per_sm = 0;
   uint64_t wave_positions = 1ull << 27;  // seed positions per batched wave
   // CUDA graph of the batched wave chain
