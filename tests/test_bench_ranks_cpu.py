@@ -53,3 +53,24 @@ def test_reference_arm_prints_only_on_rank_zero():
     with contextlib.redirect_stdout(buf):
         bench.run_reference(args, rank=1)
     assert buf.getvalue() == ""
+
+
+def test_reference_arm_prints_the_contract_line():
+    """bench.py --impl reference on a small CPU case: one JSON line with the
+    contract's keys, its cpu_baseline and e2e describing the same run."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--config", "1",
+                          "--scale", "0.05", "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=300, check=True).stdout
+    lines = [l for l in out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
