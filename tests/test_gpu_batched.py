@@ -151,3 +151,21 @@ def test_capacity_overflow_reruns_give_the_same_records(workload):
     assert got.tobytes() == base.tobytes()
     assert plain1.tobytes() == plain0.tobytes()
     assert (st1["hits"], st1["cells"], st1["raw_hsps"]) == (st0["hits"], st0["cells"], st0["raw_hsps"])
+
+
+@pytest.mark.parametrize("kw", [dict(strand="minus"), dict(strand="plus"), dict(transitions=False),
+                                dict(noentropy=True), dict(wga_chunk=30_000, interval=100_000),
+                                dict(seed="111010010100110111"), dict(max_hits=5000)])
+def test_batched_equals_plain_under_flags(workload, kw):
+    target, chunks = workload
+    chunks = chunks[:10]
+    with Engine(EngineConfig(**kw)) as e:
+        e.load_target(target)
+        e.stage_queries(chunks)
+        got, st = e.run_batched()
+        want = []
+        for i in range(len(chunks)):
+            e.select_query(i)
+            r, _ = e.run_pass()
+            want.append([tuple(int(x[f]) for f in FIELDS) for x in r])
+    assert per_query(got, len(chunks)) == want
