@@ -647,6 +647,12 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       ga.xdrop = e->cfg.xdrop;
       ga.hspthresh = e->cfg.hspthresh;
       ga.cap = e->gate_cap;
+      {
+        int32_t top = 0;  // the largest substitution score (0 if none is positive)
+        for (int i = 0; i < 64; i++) top = std::max(top, e->cfg.sub_mat[i]);
+        ga.late_max_safe = 7ll * top <= (long long)e->cfg.xdrop;
+        ga.total_exact = 2ll * (long long)e->gate_cap * top < (1ll << 24);
+      }
       ga.cand = e->cand.p;
       ga.cand_cap = e->cand_cap;
       ga.tile_first = e->tile_first.p;

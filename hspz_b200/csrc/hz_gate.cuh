@@ -14,10 +14,15 @@
 //   (3) runs the X-drop score gate thread-per-hit, first all right
 //       extensions of the tile and then all left extensions.  Before each
 //       pass the warp gathers every hit's first eight cells of both
-//       sequences (and the next word), so a lane's first step needs no global
-//       load; each lane refills from the tile when its extension ends, so
-//       extensions of different lengths do not idle the warp, and it fetches
-//       the words of its next eight cells one step ahead.
+//       sequences, so a lane's first step scores from shared memory while
+//       the words of its second step load; each lane refills from the tile
+//       when its extension ends, so extensions of different lengths do not
+//       idle the warp, and it fetches the words of its next eight cells one
+//       step ahead.
+// The kernel leans on L1: a hit's reference and query lines, brought in when
+// its first cells are gathered, serve the loads of its later steps.  So the
+// per-warp shared memory is kept small enough for four blocks per SM to
+// leave ~90 KB of L1 (with 28 KB the gate runs ~1.5x slower).
 // Anchors are the END of the seed window on both sides (pos + seed_size,
 // src/gpu/kernels.rs:397-401).  A hit becomes a candidate when
 // (i32)(f32)(right max + left max) >= hspthresh -- the reference gate's bound
@@ -44,7 +49,6 @@ struct WarpTile {
     } setup;
     struct {
       uint4 first[TW];  // first eight cells: reference words a, b; query words a, b
-      uint2 carry[TW];  // the next reference / query word of the stream
     } pass;
   } u;
   uint32_t hit_r[TW];     // reference anchor
@@ -77,6 +81,13 @@ struct GateArgs {
   uint32_t cand_cap;
   const uint32_t *tile_first;  // first position with hits of each tile (tile_table_kernel)
   const uint32_t *tile_call;   // call of that position
+  // 7 * (largest substitution score) <= xdrop: no cell within seven cells
+  // after a dropping cell can raise the maximum, so an extension that drops
+  // inside an eight-cell group ends with the group's final maximum
+  uint32_t late_max_safe;
+  // 2 * cap * (largest substitution score) < 2^24: every gate total is exact
+  // in f32, so (i32)(f32)total >= hspthresh is total >= hspthresh
+  uint32_t total_exact;
 };
 
 __device__ __forceinline__ const uint32_t *word_ptr(const uint8_t *p) {
@@ -142,8 +153,8 @@ __device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint
 
 // Scores one cell whose byte offset into the substitution table is byte SH
 // of T (extracted, zero-extended, by one byte permute); keeps every running
-// sum S and maximum M for the termination path and the group's smallest sum.
-// Since every M_i <= M_7, no cell of the group can have dropped when
+// sum S for the termination path and the group's smallest sum.  Since every
+// running maximum M_i <= M_7, no cell of the group can have dropped when
 // M_7 - min S <= xdrop.
 #define HZ_CELL(T, SH, I)                                                            \
   {                                                                                  \
@@ -151,7 +162,6 @@ __device__ __forceinline__ void first_group(const uint8_t *seq, uint32_t p, uint
     S = (int32_t)((uint32_t)S + (uint32_t)sc);                                       \
     M = max(M, S);                                                                   \
     Si[I] = S;                                                                       \
-    Mi[I] = M;                                                                       \
     Smin = min(Smin, S);                                                             \
   }
 
@@ -167,7 +177,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
   int32_t S = 0, M = 0;
   uint32_t cells = 0;
   // word stream state: the group about to be scored (ra, rb, qa, qb), the
-  // carried word and the two prefetched words of the following group
+  // word the following group starts in and the two prefetched words after it
   uint32_t ra = 0, rb = 0, qa = 0, qb = 0;
   uint32_t rc = 0, r1 = 0, r2 = 0, qc = 0, q1 = 0, q2 = 0;
   const uint32_t *wr = nullptr, *wq = nullptr;
@@ -193,18 +203,19 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
             M = 0;
             cells = 0;
             uint4 f = wt.u.pass.first[t];
-            uint2 cw = wt.u.pass.carry[t];
             ra = f.x;
             rb = f.y;
             qa = f.z;
             qb = f.w;
-            rc = cw.x;
-            qc = cw.y;
-            sr = (r0 & 3u) * 8u;
-            sq = (q0 & 3u) * 8u;
+            sr = r0 << 3;  // the funnel shifts use the low five bits: (r0 & 3) * 8
+            sq = q0 << 3;
+            // the carried word is reloaded here rather than staged: its line
+            // is in L1 from the gather, and the smaller staging leaves L1 larger
             if (!LEFT) {
               wr = word_ptr(ref + r0) + 2;  // the carried word
               wq = word_ptr(qbuf + q0) + 2;
+              rc = __ldg(wr);
+              qc = __ldg(wq);
               r1 = __ldg(wr + 1);
               r2 = __ldg(wr + 2);
               q1 = __ldg(wq + 1);
@@ -212,6 +223,8 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
             } else {
               wr = word_ptr(ref + r0 - 8);  // the carried word
               wq = word_ptr(qbuf + q0 - 8);
+              rc = __ldg(wr);
+              qc = __ldg(wq);
               r1 = __ldg(wr - 1);
               r2 = __ldg(wr - 2);
               q1 = __ldg(wq - 1);
@@ -250,7 +263,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
       wq -= 2;
     }
     const int32_t Ms = M;
-    int32_t Si[8], Mi[8];
+    int32_t Si[8];
     int32_t Smin = S;
     HZ_CELL(ta, 0, 0)
     HZ_CELL(ta, 8, 1)
@@ -264,8 +277,12 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
     const uint32_t v = min(n, 8u);
     uint32_t dm = 0;
     if ((int32_t)((uint32_t)M - (uint32_t)Smin) > X || n <= 8) {
+      int32_t m = Ms;
 #pragma unroll
-      for (int i = 0; i < 8; i++) dm |= (uint32_t)((int32_t)((uint32_t)Mi[i] - (uint32_t)Si[i]) > X) << i;
+      for (int i = 0; i < 8; i++) {
+        m = max(m, Si[i]);
+        dm |= (uint32_t)((int32_t)((uint32_t)m - (uint32_t)Si[i]) > X) << i;
+      }
       dm &= (1u << v) - 1u;
     }
     if (!dm && n > 8) {  // no drop and more cells left: advance the stream
@@ -294,10 +311,13 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
     // M - S > xdrop (keeping the maximum from before it), or after the v
     // valid cells left before the edge or the cap.
     const uint32_t stop = dm ? (uint32_t)(__ffs(dm) - 1) : v;
-    int32_t res = Ms;
+    int32_t res = M;  // a drop, and no later cell of the group raised the maximum
+    if (!dm || !a.late_max_safe) {  // the maximum over the cells before `stop`
+      res = Ms;
 #pragma unroll
-    for (int i = 1; i <= 8; i++)
-      if ((uint32_t)i == stop) res = Mi[i - 1];
+      for (int i = 0; i < 8; i++)
+        if ((uint32_t)i < stop) res = max(res, Si[i]);
+    }
     cells += dm ? stop + 1 : v;
     const bool spill = !dm && capped;
     if (spill) {
@@ -312,7 +332,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
     } else {
       cells_acc += cells + wt.hit_rcells[t];
       int32_t total = (int32_t)((uint32_t)wt.hit_rmax[t] + (uint32_t)res);
-      if (sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
+      if (a.total_exact ? total >= a.hspthresh : sat_i32((double)__int2float_rn(total)) >= a.hspthresh) {
         uint32_t at = atomicAdd(&a.tot->cand, 1u);
         if (at < a.cand_cap)
           a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
@@ -323,8 +343,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
   }
 }
 
-// Fills the first eight cells and the carried word of every hit of the
-// warp's tile for one pass.
+// Fills the first eight cells of every hit of the warp's tile for one pass.
 template <int TW, bool LEFT>
 __device__ __forceinline__ void prepare_pass(const GateArgs &a, WarpTile<TW> &wt, uint32_t nt, uint32_t lane) {
   for (uint32_t i = lane; i < nt; i += 32) {
@@ -333,7 +352,6 @@ __device__ __forceinline__ void prepare_pass(const GateArgs &a, WarpTile<TW> &wt
     first_group<LEFT>(a.w.ref, wt.hit_r[i], &ra, &rb, &rc);
     first_group<LEFT>(a.w.qbuf, wt.hit_q[i], &qa, &qb, &qc);
     wt.u.pass.first[i] = make_uint4(ra, rb, qa, qb);
-    wt.u.pass.carry[i] = make_uint2(rc, qc);
   }
 }
 

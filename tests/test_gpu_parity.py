@@ -147,12 +147,36 @@ def test_flag_variants_parity(kw):
         okw["noentropy"] = True
     if "strand" in okw:
         okw["strand"] = {"plus": 1, "minus": 2, "both": 3}[okw["strand"]]
-    want, _ = oracle_run(t, q, sm, **okw)
+    want, st_o = oracle_run(t, q, sm, **okw)
     with engine_for(sm, **kw) as e:
         e.load_target(t)
         e.swap_query_ascii(q)
-        got, _ = e.run_pass()
+        got, st = e.run_pass()
     assert got.tobytes() == want.tobytes()
+    # xdrop 500 < 7 * 100: an extension dropping inside a group may not end with
+    # the group's final maximum, so the gate takes its general path there
+    assert (st["hits"], st["raw_hsps"], st["cells"]) == (st_o["hits"], st_o["raw_hsps"], st_o["cells"])
+
+
+@pytest.mark.parametrize("cap", [128, 1024])
+def test_scaled_matrix_parity(cap):
+    """Scores, xdrop and threshold x 1000: gate totals can pass 2^24, where
+    (i32)(f32)total may differ from total, so the gate rounds through f32."""
+    t, q = synth.config1(seed=17, scale=0.1)
+    sm = [v * 1000 for v in EngineConfig().sub_mat]
+    want, st_o = oracle_run(t, q, sm, xdrop=910_000, hspthresh=3_000_000)
+    with engine_for(sm, xdrop=910_000, hspthresh=3_000_000) as e:
+        e.set_tuning(gate_cap=cap)
+        e.load_target(t)
+        e.swap_query_ascii(q)
+        got, st = e.run_pass()
+        e.stage_queries([q])
+        bgot, bst = e.run_batched()
+    assert len(want) > 0
+    assert got.tobytes() == want.tobytes()
+    assert (st["hits"], st["raw_hsps"], st["cells"]) == (st_o["hits"], st_o["raw_hsps"], st_o["cells"])
+    fields = ("interval", "strand", "ref_start", "query_start", "len", "score")
+    assert all((bgot[f] == got[f]).all() for f in fields) and bst["cells"] == st["cells"]
 
 
 def test_single_call_uploaded_vs_generated_seeds():
