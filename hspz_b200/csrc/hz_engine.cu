@@ -165,39 +165,55 @@ int parse_shape(const char *spec, ShapeDev *sh) {
 }
 
 // --- dedup_and_order (src/hsp.rs:62-126) --------------------------------------
+// by_diagonal: diagonal, ref_start, len ascending, score descending;
+// by_lastz: query_start, ref_start, len ascending, score descending.
 inline uint32_t diag_of(const hz_segment_pair &h) { return h.ref_start - h.query_start; }
-bool by_diagonal(const hz_segment_pair &x, const hz_segment_pair &y) {
-  uint32_t dx = diag_of(x), dy = diag_of(y);
-  if (dx != dy) return dx < dy;
-  if (x.ref_start != y.ref_start) return x.ref_start < y.ref_start;
-  if (x.len != y.len) return x.len < y.len;
-  return x.score > y.score;
-}
-bool by_lastz(const hz_segment_pair &x, const hz_segment_pair &y) {
-  if (x.query_start != y.query_start) return x.query_start < y.query_start;
-  if (x.ref_start != y.ref_start) return x.ref_start < y.ref_start;
-  if (x.len != y.len) return x.len < y.len;
-  return x.score > y.score;
-}
 bool contained(const hz_segment_pair &x, const hz_segment_pair &y) {
   uint32_t xe = x.ref_start + x.len, ye = y.ref_start + y.len;
   return diag_of(x) == diag_of(y) &&
          ((x.ref_start >= y.ref_start && xe <= ye) || (y.ref_start >= x.ref_start && ye <= xe));
 }
-// Both orders are total over the four fields, so std::sort reproduces the
-// reference's stable sorts exactly.
+// Both orders are total over the four fields, so any sort reproduces the
+// reference's stable sorts exactly.  Each record is sorted as one 128-bit key
+// whose unsigned order is the comparator's (score flipped for descending);
+// the record is recovered from the key, since the fields determine it.
+typedef unsigned __int128 u128;
+inline uint32_t score_desc(int32_t s) { return ~((uint32_t)s ^ 0x80000000u); }
+inline int32_t score_of(uint32_t k) { return (int32_t)(~k ^ 0x80000000u); }
+inline u128 key4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return ((u128)a << 96) | ((u128)b << 64) | ((u128)c << 32) | (u128)d;
+}
 size_t dedup_and_order(hz_segment_pair *h, size_t n) {
   if (n == 0) return 0;
-  std::sort(h, h + n, by_diagonal);
-  size_t k = 1;
-  hz_segment_pair prev = h[0];
+  std::vector<u128> key(n);
+  for (size_t i = 0; i < n; i++) key[i] = key4(diag_of(h[i]), h[i].ref_start, h[i].len, score_desc(h[i].score));
+  std::sort(key.begin(), key.end());  // by_diagonal
+  auto rec = [](u128 k) {
+    hz_segment_pair r;
+    uint32_t diag = (uint32_t)(k >> 96);
+    r.ref_start = (uint32_t)(k >> 64);
+    r.query_start = r.ref_start - diag;
+    r.len = (uint32_t)(k >> 32);
+    r.score = score_of((uint32_t)k);
+    return r;
+  };
+  size_t m = 1;
+  hz_segment_pair prev = rec(key[0]);
+  key[0] = key4(prev.query_start, prev.ref_start, prev.len, score_desc(prev.score));
   for (size_t i = 1; i < n; i++) {
-    hz_segment_pair cur = h[i];
-    if (!contained(prev, cur)) h[k++] = cur;
+    hz_segment_pair cur = rec(key[i]);
+    if (!contained(prev, cur)) key[m++] = key4(cur.query_start, cur.ref_start, cur.len, score_desc(cur.score));
     prev = cur;
   }
-  std::sort(h, h + k, by_lastz);
-  return k;
+  std::sort(key.begin(), key.begin() + m);  // by_lastz
+  for (size_t i = 0; i < m; i++) {
+    u128 k = key[i];
+    h[i].query_start = (uint32_t)(k >> 96);
+    h[i].ref_start = (uint32_t)(k >> 64);
+    h[i].len = (uint32_t)(k >> 32);
+    h[i].score = score_of((uint32_t)k);
+  }
+  return m;
 }
 
 unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148u * 64u) {
@@ -437,7 +453,8 @@ template <int TW> int launch_gate(hz_engine *e, const GateArgs &ga) {
 // the uploaded seed array of a single-call wave, or null.
 // dedup_and_order of every scope of a wave on the device (hz_dedup.cuh);
 // appends the kept HSPs, in scope order and LASTZ order within each scope.
-int dedup_on_device(hz_engine *e, uint32_t nraw, uint32_t n_scopes, std::vector<WaveRecord> *out, hz_stats *st) {
+int dedup_on_device(hz_engine *e, uint32_t nraw, uint32_t n_scopes, uint32_t call_base, std::vector<WaveRecord> *out,
+                    hz_stats *st) {
   cudaStream_t s = e->st;
   TRY(e->d_perm_a.ensure(nraw, s));
   TRY(e->d_perm_b.ensure(nraw, s));
@@ -502,7 +519,7 @@ int dedup_on_device(hz_engine *e, uint32_t nraw, uint32_t n_scopes, std::vector<
   TRY(e->sync());
   for (uint32_t i = 0; i < kept; i++) {
     const ScopedHspOut &r = e->h_out.p[i];
-    out->push_back(WaveRecord{e->h_scope_call.p[r.scope],
+    out->push_back(WaveRecord{e->h_scope_call.p[r.scope] + call_base,
                               hz_segment_pair{r.h.ref_start, r.h.query_start, r.h.len, r.h.score}});
   }
   if (st) st->hsps += kept;
@@ -553,8 +570,52 @@ template <typename F> int run_captured(hz_engine *e, F &&chain) {
   return HZ_OK;
 }
 
+// The host side of a wave's dedup: the wave's raw HSPs and their scopes,
+// already read back into e->h_raw / h_raw_scope / h_scope_call, are grouped by
+// scope and deduped per scope; the records go to *out in scope order, with
+// their wave-relative call index plus `call_base`.
+void host_dedup(hz_engine *e, uint32_t nraw, uint32_t n_scopes, uint32_t call_base, std::vector<WaveRecord> *out,
+                hz_stats *st) {
+  // counting sort by scope
+  std::vector<uint32_t> start(n_scopes + 1, 0);
+  for (uint32_t i = 0; i < nraw; i++) start[e->h_raw_scope.p[i] + 1]++;
+  for (uint32_t k = 0; k < n_scopes; k++) start[k + 1] += start[k];
+  std::vector<hz_segment_pair> sorted(nraw);
+  std::vector<uint32_t> cur(start.begin(), start.end() - 1);
+  for (uint32_t i = 0; i < nraw; i++) sorted[cur[e->h_raw_scope.p[i]]++] = e->h_raw.p[i];
+  for (uint32_t k = 0; k < n_scopes; k++) {
+    size_t a = start[k], b = start[k + 1];
+    if (a == b) continue;
+    size_t kept = dedup_and_order(sorted.data() + a, b - a);
+    if (st) st->hsps += kept;
+    uint32_t c = e->h_scope_call.p[k] + call_base;
+    for (size_t i = 0; i < kept; i++) out->push_back(WaveRecord{c, sorted[a + i]});
+  }
+}
+
+// A wave whose host dedup is still to run.  The plain form hands it to the
+// next call's run_wave, which runs it after launching its own kernels, so the
+// host sort overlaps the device work.  The engine's host read-back buffers
+// stay untouched until then: the next wave refills them only after its sync.
+struct DeferredDedup {
+  bool pending = false;
+  uint32_t nraw = 0, n_scopes = 0, call_base = 0;
+  std::vector<WaveRecord> *out = nullptr;
+  hz_stats *st = nullptr;
+  void finish(hz_engine *e) {
+    if (!pending) return;
+    pending = false;
+    host_dedup(e, nraw, n_scopes, call_base, out, st);
+  }
+};
+
+// With `defer`, a wave deduped on the host leaves that step in *defer (see
+// DeferredDedup) and the records of an earlier deferred wave are emitted once
+// this wave's kernels are queued; `call_base` is added to the call index of
+// every record the wave emits.
 int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, int transitions,
-             std::vector<WaveRecord> *out, hz_stats *st, bool device_dedup, bool graph = false) {
+             std::vector<WaveRecord> *out, hz_stats *st, bool device_dedup, bool graph = false,
+             DeferredDedup *defer = nullptr, uint32_t call_base = 0) {
   if (n == 0) return HZ_OK;
   cudaStream_t s = e->st;
   uint64_t npos = 0;
@@ -685,6 +746,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     };
     if (graph) TRY(run_captured(e, chain));
     else TRY(chain());
+    if (defer) defer->finish(e);  // the previous call's host dedup, while this call's kernels run
     TRY(e->sync());
     WaveTotals t = *e->h_tot.p;
     if (t.status & 2u) return fail(HZ_E_INVALID, "a call holds 2^32 or more seed hits; num_hits is a u32 in the reference");
@@ -723,7 +785,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     // per-call waves (the plain form) dedup on the host like the reference,
     // unless the call holds so many raw HSPs that the device sort is faster
     if (device_dedup || (e->device_dedup && nraw >= e->device_dedup_min))
-      return dedup_on_device(e, nraw, t.n_scopes, out, st);
+      return dedup_on_device(e, nraw, t.n_scopes, call_base, out, st);
     TRY(e->h_raw.ensure(nraw));
     TRY(e->h_raw_scope.ensure(nraw));
     TRY(e->h_scope_call.ensure(t.n_scopes + 1));
@@ -731,21 +793,16 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     CK(cudaMemcpyAsync(e->h_raw_scope.p, e->raw_scope.p, (size_t)nraw * 4, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(e->h_scope_call.p, e->scope_call.p, (size_t)t.n_scopes * 4, cudaMemcpyDeviceToHost, s));
     TRY(e->sync());
-    // counting sort by scope
-    std::vector<uint32_t> start(t.n_scopes + 1, 0);
-    for (uint32_t i = 0; i < nraw; i++) start[e->h_raw_scope.p[i] + 1]++;
-    for (uint32_t k = 0; k < t.n_scopes; k++) start[k + 1] += start[k];
-    std::vector<hz_segment_pair> sorted(nraw);
-    std::vector<uint32_t> cur(start.begin(), start.end() - 1);
-    for (uint32_t i = 0; i < nraw; i++) sorted[cur[e->h_raw_scope.p[i]]++] = e->h_raw.p[i];
-    for (uint32_t k = 0; k < t.n_scopes; k++) {
-      size_t a = start[k], b = start[k + 1];
-      if (a == b) continue;
-      size_t kept = dedup_and_order(sorted.data() + a, b - a);
-      if (st) st->hsps += kept;
-      uint32_t c = e->h_scope_call.p[k];
-      for (size_t i = 0; i < kept; i++) out->push_back(WaveRecord{c, sorted[a + i]});
+    if (defer) {
+      defer->pending = true;
+      defer->nraw = nraw;
+      defer->n_scopes = t.n_scopes;
+      defer->call_base = call_base;
+      defer->out = out;
+      defer->st = st;
+      return HZ_OK;
     }
+    host_dedup(e, nraw, t.n_scopes, call_base, out, st);
     return HZ_OK;
   }
   return fail(HZ_E_OOM, "wave buffers kept overflowing");
@@ -1313,11 +1370,10 @@ int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats
   std::vector<HostCall> calls;
   query_calls(e, e->cur_query, &calls);
   std::vector<WaveRecord> recs;
-  for (size_t i = 0; i < calls.size(); i++) {
-    size_t before = recs.size();
-    TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local, false));
-    for (size_t k = before; k < recs.size(); k++) recs[k].call = (uint32_t)i;  // wave-relative -> pass call
-  }
+  DeferredDedup defer;  // call i's host dedup runs while call i + 1's kernels do
+  for (size_t i = 0; i < calls.size(); i++)
+    TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local, false, false, &defer, (uint32_t)i));
+  defer.finish(e);
   // records of one interval: plus calls before minus calls (call order already)
   if (!recs.empty()) {
     *out = (hz_pass_record *)malloc(recs.size() * sizeof(hz_pass_record));

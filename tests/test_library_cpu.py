@@ -69,6 +69,16 @@ def test_library_dedup_matches_oracle():
         got = E.dedup_and_order(a)
         want = oracle.dedup_and_order(a)
         assert got.tobytes() == want.tobytes()
+    # field extremes: coordinates near 2^32 (wrapping ends) and scores at both
+    # ends of i32, which the library's sort keys flip for descending order
+    for n in [64, 3000]:
+        a = np.zeros(n, dtype=oracle.HSP_DTYPE)
+        edge = np.array([0, 1, 2, 0xFFFFFFFD, 0xFFFFFFFE, 0xFFFFFFFF], dtype=np.uint64)
+        a["ref_start"] = rng.choice(edge, n)
+        a["query_start"] = rng.choice(edge, n)
+        a["len"] = rng.choice(np.array([0, 1, 2, 0xFFFFFFFF], dtype=np.uint64), n)
+        a["score"] = rng.choice(np.array([-2**31, -2**31 + 1, -1, 0, 1, 2**31 - 2, 2**31 - 1]), n)
+        assert E.dedup_and_order(a).tobytes() == oracle.dedup_and_order(a).tobytes()
     # wrapping diagonal: query start beyond ref start sorts last (src/hsp.rs:298-303)
     a = np.array([(4, 10, 0, 0), (10, 4, 0, 0)], dtype=oracle.HSP_DTYPE)
     assert E.dedup_and_order(a).tolist() == [(10, 4, 0, 0), (4, 10, 0, 0)]
