@@ -597,6 +597,10 @@ void host_dedup(hz_engine *e, uint32_t nraw, uint32_t n_scopes, uint32_t call_ba
 // next call's run_wave, which runs it after launching its own kernels, so the
 // host sort overlaps the device work.  The engine's host read-back buffers
 // stay untouched until then: the next wave refills them only after its sync.
+// Raw HSPs and scopes a plain call reads back with its totals (40 KB).
+constexpr uint32_t kRawPrefix = 2048;
+constexpr uint32_t kScopePrefix = 64;
+
 struct DeferredDedup {
   bool pending = false;
   uint32_t nraw = 0, n_scopes = 0, call_base = 0;
@@ -747,6 +751,19 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     if (graph) TRY(run_captured(e, chain));
     else TRY(chain());
     if (defer) defer->finish(e);  // the previous call's host dedup, while this call's kernels run
+    // A plain call reads back the first raw HSPs and scopes with its totals,
+    // so one with few raw HSPs (the usual case) needs one sync, not two.
+    uint32_t pre_raw = 0, pre_scopes = 0;
+    if (defer) {
+      pre_raw = std::min<uint32_t>(kRawPrefix, e->raw_cap);
+      pre_scopes = std::min<uint32_t>(kScopePrefix, scope_cap + 1);
+      TRY(e->h_raw.ensure(pre_raw));
+      TRY(e->h_raw_scope.ensure(pre_raw));
+      TRY(e->h_scope_call.ensure(pre_scopes));
+      CK(cudaMemcpyAsync(e->h_raw.p, e->raw.p, (size_t)pre_raw * sizeof(SegmentPair), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(e->h_raw_scope.p, e->raw_scope.p, (size_t)pre_raw * 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(e->h_scope_call.p, e->scope_call.p, (size_t)pre_scopes * 4, cudaMemcpyDeviceToHost, s));
+    }
     TRY(e->sync());
     WaveTotals t = *e->h_tot.p;
     if (t.status & 2u) return fail(HZ_E_INVALID, "a call holds 2^32 or more seed hits; num_hits is a u32 in the reference");
@@ -786,13 +803,15 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     // unless the call holds so many raw HSPs that the device sort is faster
     if (device_dedup || (e->device_dedup && nraw >= e->device_dedup_min))
       return dedup_on_device(e, nraw, t.n_scopes, call_base, out, st);
-    TRY(e->h_raw.ensure(nraw));
-    TRY(e->h_raw_scope.ensure(nraw));
-    TRY(e->h_scope_call.ensure(t.n_scopes + 1));
-    CK(cudaMemcpyAsync(e->h_raw.p, e->raw.p, (size_t)nraw * sizeof(SegmentPair), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_raw_scope.p, e->raw_scope.p, (size_t)nraw * 4, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_scope_call.p, e->scope_call.p, (size_t)t.n_scopes * 4, cudaMemcpyDeviceToHost, s));
-    TRY(e->sync());
+    if (nraw > pre_raw || t.n_scopes > pre_scopes) {  // not all read back with the totals
+      TRY(e->h_raw.ensure(nraw));
+      TRY(e->h_raw_scope.ensure(nraw));
+      TRY(e->h_scope_call.ensure(t.n_scopes + 1));
+      CK(cudaMemcpyAsync(e->h_raw.p, e->raw.p, (size_t)nraw * sizeof(SegmentPair), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(e->h_raw_scope.p, e->raw_scope.p, (size_t)nraw * 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(e->h_scope_call.p, e->scope_call.p, (size_t)t.n_scopes * 4, cudaMemcpyDeviceToHost, s));
+      TRY(e->sync());
+    }
     if (defer) {
       defer->pending = true;
       defer->nraw = nraw;
