@@ -8,6 +8,7 @@
 // its HSPs back after each call, as the reference does; the batched form runs
 // many calls per wave with one read-back per wave.
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -301,6 +302,9 @@ struct hz_engine {
   } build;
   bool has_target = false;
   bool owns_target = true;         // false for serving workers that share the owner's tables
+  bool aliases_query = false;      // true for the plain form's second workspace (see run_pass_two)
+  hz_engine *twin = nullptr;       // that workspace, made on first use
+  int plain_streams = 2;           // host threads / streams of a plain pass (1 or 2)
   struct Server *server = nullptr;  // the serving loop, while one runs
   // query store
   SeqBuf qstore;
@@ -751,10 +755,11 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
     if (graph) TRY(run_captured(e, chain));
     else TRY(chain());
     if (defer) defer->finish(e);  // the previous call's host dedup, while this call's kernels run
-    // A plain call reads back the first raw HSPs and scopes with its totals,
-    // so one with few raw HSPs (the usual case) needs one sync, not two.
+    // A single-call wave (the plain form) reads back the first raw HSPs and
+    // scopes with its totals, so one with few raw HSPs (the usual case) needs
+    // one sync, not two.
     uint32_t pre_raw = 0, pre_scopes = 0;
-    if (defer) {
+    if (n == 1 && !device_dedup) {
       pre_raw = std::min<uint32_t>(kRawPrefix, e->raw_cap);
       pre_scopes = std::min<uint32_t>(kScopePrefix, scope_cap + 1);
       TRY(e->h_raw.ensure(pre_raw));
@@ -1036,13 +1041,17 @@ void hz_engine_destroy(hz_engine *e) {
   cudaSetDevice(e->device);
   if (e->st) cudaStreamSynchronize(e->st);
   if (e->server) hz_serve_stop(e);
+  if (e->twin) {
+    hz_engine_destroy(e->twin);
+    e->twin = nullptr;
+  }
   if (e->owns_target) {
     e->ref.buf.release();
     e->index_table.release();
     e->pos_table.release();
     e->nbr_hits.release();
   }
-  e->qstore.buf.release();
+  if (!e->aliases_query) e->qstore.buf.release();
   e->qascii.release();
   e->build.release();
   for (auto &s : e->slot) s.seeds.release();
@@ -1375,6 +1384,94 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
   return HZ_OK;
 }
 
+namespace {
+void share_target(hz_engine *w, const hz_engine *e);
+int clone_shared(hz_engine *e, hz_engine **out);
+
+void add_stats(hz_stats *a, const hz_stats &b) {
+  a->seeds += b.seeds;
+  a->hits += b.hits;
+  a->raw_hsps += b.raw_hsps;
+  a->hsps += b.hsps;
+  a->cells += b.cells;
+  a->calls += b.calls;
+}
+
+// The plain pass over two workspaces: this engine and a second one (its own
+// stream and wave buffers over the same target tables and query store), each
+// driven by its own host thread and taking the next call from a shared
+// counter.  While one waits for its call's read-back and dedups it on the
+// host, the other's kernels run, so the device is not idle between calls.
+// Calls are independent, so each call's records are the same as on one
+// workspace; they are put back in call order.
+int run_pass_two(hz_engine *e, const std::vector<HostCall> &calls, std::vector<WaveRecord> *recs, hz_stats *st) {
+  if (!e->twin) {
+    TRY(clone_shared(e, &e->twin));
+    e->twin->qstore.buf.release();  // it uses this engine's query store instead
+    e->twin->aliases_query = true;
+  }
+  hz_engine *w = e->twin;
+  share_target(w, e);  // the target, configuration and knobs may have changed since the last pass
+  w->qstore.buf.p = e->qstore.buf.p;
+  w->qstore.buf.cap = e->qstore.buf.cap;
+  w->qstore.len = e->qstore.len;
+  w->queries = e->queries;
+  w->cur_query = e->cur_query;
+  w->has_query = e->has_query;
+  w->profiling = e->profiling;
+  const uint64_t w_launches = w->launches;
+
+  std::vector<std::vector<WaveRecord>> per(calls.size());
+  std::atomic<size_t> next{0};
+  std::atomic<bool> stop{false};
+  auto drive = [&](hz_engine *x, hz_stats *sx) -> int {
+    for (;;) {
+      if (stop.load()) return HZ_OK;
+      size_t i = next.fetch_add(1);
+      if (i >= calls.size()) return HZ_OK;
+      int rc = run_wave(x, &calls[i], 1, nullptr, x->cfg.transitions, &per[i], sx, false, false, nullptr, (uint32_t)i);
+      if (rc != HZ_OK) {
+        stop.store(true);
+        return rc;
+      }
+    }
+  };
+  hz_stats st_w;
+  memset(&st_w, 0, sizeof st_w);
+  int rc_w = HZ_OK;
+  std::string err_w;
+  std::thread helper([&] {
+    if (cudaSetDevice(w->device) != cudaSuccess) {
+      rc_w = HZ_E_CUDA;
+      err_w = "second plain workspace: cudaSetDevice failed";
+      stop.store(true);
+      return;
+    }
+    rc_w = drive(w, &st_w);
+    if (rc_w != HZ_OK) err_w = g_err;
+  });
+  int rc = drive(e, st);
+  helper.join();
+  // the second workspace's kernels and profile count as this engine's
+  e->launches += w->launches - w_launches;
+  for (const std::string &k : w->prof_order) {
+    if (!e->prof.count(k)) e->prof_order.push_back(k);
+    e->prof[k].ms += w->prof[k].ms;
+    e->prof[k].n += w->prof[k].n;
+  }
+  w->prof.clear();
+  w->prof_order.clear();
+  if (rc != HZ_OK) return rc;
+  if (rc_w != HZ_OK) return fail(rc_w, "%s", err_w.c_str());
+  add_stats(st, st_w);
+  size_t total = 0;
+  for (auto &v : per) total += v.size();
+  recs->reserve(total);
+  for (auto &v : per) recs->insert(recs->end(), v.begin(), v.end());
+  return HZ_OK;
+}
+}  // namespace
+
 // The plain per-chunk form: one wave (launch chain + read-back + host dedup)
 // per seed_and_filter call, in the reference's call order.
 int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats) {
@@ -1389,10 +1486,15 @@ int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats
   std::vector<HostCall> calls;
   query_calls(e, e->cur_query, &calls);
   std::vector<WaveRecord> recs;
-  DeferredDedup defer;  // call i's host dedup runs while call i + 1's kernels do
-  for (size_t i = 0; i < calls.size(); i++)
-    TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local, false, false, &defer, (uint32_t)i));
-  defer.finish(e);
+  // (on a caller's stream, every call stays on that stream)
+  if (e->plain_streams >= 2 && calls.size() >= 2 && e->st == e->own_st) {
+    TRY(run_pass_two(e, calls, &recs, &local));
+  } else {
+    DeferredDedup defer;  // call i's host dedup runs while call i + 1's kernels do
+    for (size_t i = 0; i < calls.size(); i++)
+      TRY(run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &recs, &local, false, false, &defer, (uint32_t)i));
+    defer.finish(e);
+  }
   // records of one interval: plus calls before minus calls (call order already)
   if (!recs.empty()) {
     *out = (hz_pass_record *)malloc(recs.size() * sizeof(hz_pass_record));
@@ -1731,6 +1833,9 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   } else if (k == "wave_positions") {
     if (value < 1 || value >= (1ll << 31)) return fail(HZ_E_INVALID, "wave_positions must be 1..2^31-1");
     e->wave_positions = (uint64_t)value;
+  } else if (k == "plain_streams") {
+    if (value != 1 && value != 2) return fail(HZ_E_INVALID, "plain_streams must be 1 or 2");
+    e->plain_streams = (int)value;
   } else if (k == "tile_cap" || k == "cand_cap" || k == "raw_cap") {
     // starting capacities; a wave that needs more grows them and runs again
     if (value < 16 || value > 0x7FFFFFFFll) return fail(HZ_E_INVALID, "%s must be 16..2^31-1", key);
@@ -1889,9 +1994,9 @@ namespace {
 // candidate, HSP and dedup buffers.
 uint64_t serve_estimate(uint64_t len) { return 2 * len * (1 + 4 + 12) + (1ull << 20); }
 
-// A workspace that shares `e`'s resident target tables without owning them.
-int clone_shared(hz_engine *e, hz_engine **out) {
-  hz_engine *w = new hz_engine();
+// Copies into `w` what a workspace shares with `e`: the resident target
+// tables (borrowed, not owned), the configuration and the launch knobs.
+void share_target(hz_engine *w, const hz_engine *e) {
   w->device = e->device;
   w->sm_count = e->sm_count;
   w->cfg = e->cfg;
@@ -1919,6 +2024,12 @@ int clone_shared(hz_engine *e, hz_engine **out) {
   w->device_dedup = e->device_dedup;
   w->device_dedup_min = e->device_dedup_min;
   w->use_graph = e->use_graph;
+}
+
+// A workspace that shares `e`'s resident target tables without owning them.
+int clone_shared(hz_engine *e, hz_engine **out) {
+  hz_engine *w = new hz_engine();
+  share_target(w, e);
   cudaError_t err = cudaStreamCreateWithFlags(&w->own_st, cudaStreamNonBlocking);
   if (err != cudaSuccess) {
     w->owns_target = false;

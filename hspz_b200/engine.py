@@ -208,7 +208,8 @@ class Engine:
 
     def set_tuning(self, **knobs):
         """Launch-shape knobs: gate_tile, gate_cap, gate_blocks_per_sm,
-        wave_positions, device_dedup, graph.  Results never depend on them."""
+        wave_positions, device_dedup, graph, plain_streams.  Results never
+        depend on them."""
         for k, v in knobs.items():
             N.check(N.lib().hz_engine_set_tuning(self._h, k.encode(), int(v)))
 

@@ -227,6 +227,11 @@ int hz_engine_profile_reset(hz_engine *e);
  * host, as the reference does),
  * "graph" (1: the batched form captures each wave's kernel chain as a CUDA
  * graph and replays it, updating the instantiated graph in place),
+ * "plain_streams" (2, the default: hz_run_pass runs its calls on this engine
+ * and a second workspace over the same target, each with its own host thread
+ * and stream, so one call's read-back and host dedup overlap another's
+ * kernels; 1: one call at a time on this engine; an engine given a caller's
+ * stream by hz_engine_set_stream runs every call on that stream),
  * "tile_cap" / "cand_cap" / "raw_cap" (starting capacities of the gate's
  * tile table, the candidate list and the raw-HSP list; a wave that needs more
  * grows them and runs again). */

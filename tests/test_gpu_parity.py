@@ -109,6 +109,38 @@ def test_config1_full_parity():
         assert st[k] == st_o[k], k
 
 
+def test_plain_pass_on_one_and_two_streams():
+    """The plain pass runs its calls over two workspaces (two host threads and
+    streams) by default; on one it must give the same records, statistics,
+    kernel launches and profiled kernels, also after the target and the query
+    change between passes."""
+    sm = EngineConfig().sub_mat
+    t1, q1 = synth.config1(seed=21, scale=0.2)
+    t2, q2 = synth.config1(seed=22, scale=0.15)
+    with engine_for(sm, wga_chunk=20_000) as e:
+        runs = {}
+        for streams in (1, 2):
+            e.set_tuning(plain_streams=streams)
+            out = []
+            for t, q in ((t1, q1), (t2, q2)):
+                e.load_target(t)
+                e.swap_query_ascii(q)
+                e.set_profiling(True)
+                e.profile_reset()
+                l0 = e.launches
+                got, st = e.run_pass()
+                prof = {k: v[1] for k, v in e.profile().items()}
+                e.set_profiling(False)
+                out.append((got.tobytes(), st, e.launches - l0, prof))
+            runs[streams] = out
+    assert st["calls"] >= 10
+    for one, two in zip(runs[1], runs[2]):
+        assert one[0] == two[0] and one[1] == two[1]
+        assert one[2] == two[2] and one[3] == two[3]
+    want, _ = oracle_run(t2, q2, sm, wga_chunk=20_000)
+    assert runs[2][1][0] == want.tobytes()
+
+
 @pytest.mark.parametrize("max_hits", [1000, 37, 250_000])
 def test_max_hits_chunking_parity(max_hits):
     """Small MAX_HITS forces the lower_bound walk (chunk_limits,
