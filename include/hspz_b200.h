@@ -126,7 +126,9 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
 
 /* seed_and_filter_all (src/run.rs:266-495), plain per-chunk form: every
  * interval x strand x WGA chunk of the swapped-in query, one launch chain per
- * call.  Records are grouped per interval, plus before minus, in call order. */
+ * call.  Records are grouped per interval, plus before minus, in call order.
+ * By default the calls run on two workspaces at once (tuning knob
+ * "plain_streams"); the records do not depend on it. */
 int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats);
 
 /* One query block for the batched form (ASCII, records joined by '&'). */
