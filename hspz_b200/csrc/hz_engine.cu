@@ -302,9 +302,9 @@ struct hz_engine {
   } build;
   bool has_target = false;
   bool owns_target = true;         // false for serving workers that share the owner's tables
-  bool aliases_query = false;      // true for the plain form's second workspace (see run_pass_two)
-  hz_engine *twin = nullptr;       // that workspace, made on first use
-  int plain_streams = 2;           // host threads / streams of a plain pass (1 or 2)
+  bool aliases_query = false;      // true for the plain form's extra workspaces (see run_pass_multi)
+  std::vector<hz_engine *> twins;  // those workspaces, made on first use
+  int plain_streams = 4;           // workspaces (host threads and streams) of a plain pass, 1..4
   struct Server *server = nullptr;  // the serving loop, while one runs
   // query store
   SeqBuf qstore;
@@ -1041,10 +1041,8 @@ void hz_engine_destroy(hz_engine *e) {
   cudaSetDevice(e->device);
   if (e->st) cudaStreamSynchronize(e->st);
   if (e->server) hz_serve_stop(e);
-  if (e->twin) {
-    hz_engine_destroy(e->twin);
-    e->twin = nullptr;
-  }
+  for (hz_engine *w : e->twins) hz_engine_destroy(w);
+  e->twins.clear();
   if (e->owns_target) {
     e->ref.buf.release();
     e->index_table.release();
@@ -1397,29 +1395,37 @@ void add_stats(hz_stats *a, const hz_stats &b) {
   a->calls += b.calls;
 }
 
-// The plain pass over two workspaces: this engine and a second one (its own
-// stream and wave buffers over the same target tables and query store), each
-// driven by its own host thread and taking the next call from a shared
-// counter.  While one waits for its call's read-back and dedups it on the
-// host, the other's kernels run, so the device is not idle between calls.
+// The plain pass over `k` workspaces: this engine and k - 1 more (each with
+// its own stream and wave buffers over the same target tables and query
+// store), each driven by its own host thread and taking the next call from a
+// shared counter.  While one waits for its call's read-back and dedups it on
+// the host, the others' kernels run, so the device is not idle between calls.
 // Calls are independent, so each call's records are the same as on one
 // workspace; they are put back in call order.
-int run_pass_two(hz_engine *e, const std::vector<HostCall> &calls, std::vector<WaveRecord> *recs, hz_stats *st) {
-  if (!e->twin) {
-    TRY(clone_shared(e, &e->twin));
-    e->twin->qstore.buf.release();  // it uses this engine's query store instead
-    e->twin->aliases_query = true;
+int run_pass_multi(hz_engine *e, int k, const std::vector<HostCall> &calls, std::vector<WaveRecord> *recs,
+                   hz_stats *st) {
+  while ((int)e->twins.size() < k - 1) {
+    hz_engine *w = nullptr;
+    TRY(clone_shared(e, &w));
+    w->qstore.buf.release();  // it uses this engine's query store instead
+    w->aliases_query = true;
+    e->twins.push_back(w);
   }
-  hz_engine *w = e->twin;
-  share_target(w, e);  // the target, configuration and knobs may have changed since the last pass
-  w->qstore.buf.p = e->qstore.buf.p;
-  w->qstore.buf.cap = e->qstore.buf.cap;
-  w->qstore.len = e->qstore.len;
-  w->queries = e->queries;
-  w->cur_query = e->cur_query;
-  w->has_query = e->has_query;
-  w->profiling = e->profiling;
-  const uint64_t w_launches = w->launches;
+  std::vector<hz_engine *> ws{e};
+  for (int j = 0; j < k - 1; j++) {
+    hz_engine *w = e->twins[j];
+    share_target(w, e);  // the target, configuration and knobs may have changed since the last pass
+    w->qstore.buf.p = e->qstore.buf.p;
+    w->qstore.buf.cap = e->qstore.buf.cap;
+    w->qstore.len = e->qstore.len;
+    w->queries = e->queries;
+    w->cur_query = e->cur_query;
+    w->has_query = e->has_query;
+    w->profiling = e->profiling;
+    ws.push_back(w);
+  }
+  std::vector<uint64_t> launches0(ws.size());
+  for (size_t j = 0; j < ws.size(); j++) launches0[j] = ws[j]->launches;
 
   std::vector<std::vector<WaveRecord>> per(calls.size());
   std::atomic<size_t> next{0};
@@ -1436,34 +1442,40 @@ int run_pass_two(hz_engine *e, const std::vector<HostCall> &calls, std::vector<W
       }
     }
   };
-  hz_stats st_w;
-  memset(&st_w, 0, sizeof st_w);
-  int rc_w = HZ_OK;
-  std::string err_w;
-  std::thread helper([&] {
-    if (cudaSetDevice(w->device) != cudaSuccess) {
-      rc_w = HZ_E_CUDA;
-      err_w = "second plain workspace: cudaSetDevice failed";
-      stop.store(true);
-      return;
+  std::vector<hz_stats> sts(ws.size());
+  for (auto &x : sts) memset(&x, 0, sizeof x);
+  std::vector<int> rcs(ws.size(), HZ_OK);
+  std::vector<std::string> errs(ws.size());
+  std::vector<std::thread> helpers;
+  for (size_t j = 1; j < ws.size(); j++)
+    helpers.emplace_back([&, j] {
+      if (cudaSetDevice(ws[j]->device) != cudaSuccess) {
+        rcs[j] = HZ_E_CUDA;
+        errs[j] = "plain workspace: cudaSetDevice failed";
+        stop.store(true);
+        return;
+      }
+      rcs[j] = drive(ws[j], &sts[j]);
+      if (rcs[j] != HZ_OK) errs[j] = g_err;
+    });
+  rcs[0] = drive(e, &sts[0]);
+  for (auto &t : helpers) t.join();
+  // the extra workspaces' kernels and profiles count as this engine's
+  for (size_t j = 1; j < ws.size(); j++) {
+    hz_engine *w = ws[j];
+    e->launches += w->launches - launches0[j];
+    for (const std::string &name : w->prof_order) {
+      if (!e->prof.count(name)) e->prof_order.push_back(name);
+      e->prof[name].ms += w->prof[name].ms;
+      e->prof[name].n += w->prof[name].n;
     }
-    rc_w = drive(w, &st_w);
-    if (rc_w != HZ_OK) err_w = g_err;
-  });
-  int rc = drive(e, st);
-  helper.join();
-  // the second workspace's kernels and profile count as this engine's
-  e->launches += w->launches - w_launches;
-  for (const std::string &k : w->prof_order) {
-    if (!e->prof.count(k)) e->prof_order.push_back(k);
-    e->prof[k].ms += w->prof[k].ms;
-    e->prof[k].n += w->prof[k].n;
+    w->prof.clear();
+    w->prof_order.clear();
   }
-  w->prof.clear();
-  w->prof_order.clear();
-  if (rc != HZ_OK) return rc;
-  if (rc_w != HZ_OK) return fail(rc_w, "%s", err_w.c_str());
-  add_stats(st, st_w);
+  if (rcs[0] != HZ_OK) return rcs[0];
+  for (size_t j = 1; j < ws.size(); j++)
+    if (rcs[j] != HZ_OK) return fail(rcs[j], "%s", errs[j].c_str());
+  for (const hz_stats &x : sts) add_stats(st, x);
   size_t total = 0;
   for (auto &v : per) total += v.size();
   recs->reserve(total);
@@ -1488,7 +1500,7 @@ int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats
   std::vector<WaveRecord> recs;
   // (on a caller's stream, every call stays on that stream)
   if (e->plain_streams >= 2 && calls.size() >= 2 && e->st == e->own_st) {
-    TRY(run_pass_two(e, calls, &recs, &local));
+    TRY(run_pass_multi(e, e->plain_streams, calls, &recs, &local));
   } else {
     DeferredDedup defer;  // call i's host dedup runs while call i + 1's kernels do
     for (size_t i = 0; i < calls.size(); i++)
@@ -1834,7 +1846,7 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
     if (value < 1 || value >= (1ll << 31)) return fail(HZ_E_INVALID, "wave_positions must be 1..2^31-1");
     e->wave_positions = (uint64_t)value;
   } else if (k == "plain_streams") {
-    if (value != 1 && value != 2) return fail(HZ_E_INVALID, "plain_streams must be 1 or 2");
+    if (value < 1 || value > 4) return fail(HZ_E_INVALID, "plain_streams must be 1..4");
     e->plain_streams = (int)value;
   } else if (k == "tile_cap" || k == "cand_cap" || k == "raw_cap") {
     // starting capacities; a wave that needs more grows them and runs again

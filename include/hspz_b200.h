@@ -127,7 +127,7 @@ int hz_seed_and_filter(hz_engine *e, uint32_t slot, int rev, hz_segment_pair **o
 /* seed_and_filter_all (src/run.rs:266-495), plain per-chunk form: every
  * interval x strand x WGA chunk of the swapped-in query, one launch chain per
  * call.  Records are grouped per interval, plus before minus, in call order.
- * By default the calls run on two workspaces at once (tuning knob
+ * By default the calls run on four workspaces at once (tuning knob
  * "plain_streams"); the records do not depend on it. */
 int hz_run_pass(hz_engine *e, hz_pass_record **out, uint64_t *n, hz_stats *stats);
 
@@ -229,11 +229,12 @@ int hz_engine_profile_reset(hz_engine *e);
  * host, as the reference does),
  * "graph" (1: the batched form captures each wave's kernel chain as a CUDA
  * graph and replays it, updating the instantiated graph in place),
- * "plain_streams" (2, the default: hz_run_pass runs its calls on this engine
- * and a second workspace over the same target, each with its own host thread
- * and stream, so one call's read-back and host dedup overlap another's
- * kernels; 1: one call at a time on this engine; an engine given a caller's
- * stream by hz_engine_set_stream runs every call on that stream),
+ * "plain_streams" (1..4, default 4: hz_run_pass runs its calls on this
+ * engine and plain_streams - 1 more workspaces over the same target, each
+ * with its own host thread and stream, so one call's read-back and host dedup
+ * overlap other calls' kernels; 1: one call at a time on this engine; an
+ * engine given a caller's stream by hz_engine_set_stream runs every call on
+ * that stream),
  * "tile_cap" / "cand_cap" / "raw_cap" (starting capacities of the gate's
  * tile table, the candidate list and the raw-HSP list; a wave that needs more
  * grows them and runs again). */

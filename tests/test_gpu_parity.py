@@ -109,17 +109,17 @@ def test_config1_full_parity():
         assert st[k] == st_o[k], k
 
 
-def test_plain_pass_on_one_and_two_streams():
-    """The plain pass runs its calls over two workspaces (two host threads and
-    streams) by default; on one it must give the same records, statistics,
-    kernel launches and profiled kernels, also after the target and the query
-    change between passes."""
+def test_plain_pass_on_one_to_four_streams():
+    """The plain pass runs its calls over several workspaces (host threads and
+    streams; four by default); on one it must give the same records,
+    statistics, kernel launches and profiled kernels, also after the target
+    and the query change between passes."""
     sm = EngineConfig().sub_mat
     t1, q1 = synth.config1(seed=21, scale=0.2)
     t2, q2 = synth.config1(seed=22, scale=0.15)
     with engine_for(sm, wga_chunk=20_000) as e:
         runs = {}
-        for streams in (1, 2):
+        for streams in (1, 2, 3, 4):
             e.set_tuning(plain_streams=streams)
             out = []
             for t, q in ((t1, q1), (t2, q2)):
@@ -134,11 +134,12 @@ def test_plain_pass_on_one_and_two_streams():
                 out.append((got.tobytes(), st, e.launches - l0, prof))
             runs[streams] = out
     assert st["calls"] >= 10
-    for one, two in zip(runs[1], runs[2]):
-        assert one[0] == two[0] and one[1] == two[1]
-        assert one[2] == two[2] and one[3] == two[3]
+    for streams in (2, 3, 4):
+        for one, many in zip(runs[1], runs[streams]):
+            assert one[0] == many[0] and one[1] == many[1], streams
+            assert one[2] == many[2] and one[3] == many[3], streams
     want, _ = oracle_run(t2, q2, sm, wga_chunk=20_000)
-    assert runs[2][1][0] == want.tobytes()
+    assert runs[4][1][0] == want.tobytes()
 
 
 @pytest.mark.parametrize("max_hits", [1000, 37, 250_000])
