@@ -1447,17 +1447,25 @@ int run_pass_multi(hz_engine *e, int k, const std::vector<HostCall> &calls, std:
   std::vector<int> rcs(ws.size(), HZ_OK);
   std::vector<std::string> errs(ws.size());
   std::vector<std::thread> helpers;
-  for (size_t j = 1; j < ws.size(); j++)
-    helpers.emplace_back([&, j] {
-      if (cudaSetDevice(ws[j]->device) != cudaSuccess) {
-        rcs[j] = HZ_E_CUDA;
-        errs[j] = "plain workspace: cudaSetDevice failed";
-        stop.store(true);
-        return;
-      }
-      rcs[j] = drive(ws[j], &sts[j]);
-      if (rcs[j] != HZ_OK) errs[j] = g_err;
-    });
+  for (size_t j = 1; j < ws.size(); j++) {
+    try {
+      helpers.emplace_back([&, j] {
+        if (cudaSetDevice(ws[j]->device) != cudaSuccess) {
+          rcs[j] = HZ_E_CUDA;
+          errs[j] = "plain workspace: cudaSetDevice failed";
+          stop.store(true);
+          return;
+        }
+        rcs[j] = drive(ws[j], &sts[j]);
+        if (rcs[j] != HZ_OK) errs[j] = g_err;
+      });
+    } catch (const std::exception &ex) {  // no thread: its workspace takes no calls
+      rcs[j] = HZ_E_OOM;
+      errs[j] = std::string("plain workspace thread: ") + ex.what();
+      stop.store(true);
+      break;
+    }
+  }
   rcs[0] = drive(e, &sts[0]);
   for (auto &t : helpers) t.join();
   // the extra workspaces' kernels and profiles count as this engine's
