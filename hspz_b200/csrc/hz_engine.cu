@@ -24,6 +24,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/hspz_b200.h"
 #include "hz_kernels.cuh"
 #include "hz_scan.cuh"
@@ -1657,21 +1659,60 @@ __global__ void na_copy_kernel(const PlainHsp *__restrict__ in, const uint32_t *
   if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = k;
 }
 
-// The scratch's device address, looked up once per device with that device
-// current (host code cannot use the symbol itself as a device pointer).
+// The unique id of the calling thread's current CUDA context (0 if there is
+// none or the driver cannot say).  Ids are never reused within a process, so
+// a context torn down and created again (cudaDeviceReset) gets a new one.
+unsigned long long current_context_id() {
+  typedef CUresult (*GetCurrentFn)(CUcontext *);
+  typedef CUresult (*GetIdFn)(CUcontext, unsigned long long *);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(p);
+    cudaGetLastError();
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
+
+// The scratch's device address, looked up with the device current (host
+// code cannot use the symbol itself as a device pointer) the first time a
+// context of that device calls, and again whenever the device's context has
+// changed since -- after a cudaDeviceReset the old address is dead.
 int noalloc_scratch(int device, uint32_t **out) {
   static uint32_t *addr[64] = {nullptr};
+  static unsigned long long ctx_of[64] = {0};
   static std::mutex mu;
   if (device < 0 || device >= 64) return fail(HZ_E_INVALID, "device %d out of range", device);
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
+  const unsigned long long ctx = current_context_id();
+  if (!addr[device] || ctx == 0 || ctx != ctx_of[device]) {
     void *p = nullptr;
     cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (err != cudaSuccess) return fail(HZ_E_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(err));
     addr[device] = static_cast<uint32_t *>(p);
+    ctx_of[device] = current_context_id();  // the lookup may have created the context
   }
   *out = addr[device];
   return HZ_OK;
+}
+
+// [a, a + na) and [b, b + nb) share a byte
+bool overlaps(const void *a, size_t na, const void *b, size_t nb) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return na && nb && x < y + nb && y < x + na;
 }
 
 }  // namespace
@@ -1686,6 +1727,11 @@ int hz_dedup_and_order_device_noalloc(const hz_segment_pair *d_in, uint32_t n, h
   if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out) |
        reinterpret_cast<uintptr_t>(d_n_out)) & 3)
     return fail(HZ_E_INVALID, "device buffers must be 4-byte aligned");
+  // the kernels read d_in while they write d_out and d_n_out, so the three
+  // must be disjoint (no in-place dedup)
+  const size_t bytes = (size_t)n * sizeof(hz_segment_pair);
+  if (overlaps(d_in, bytes, d_out, bytes) || overlaps(d_n_out, 4, d_in, bytes) || overlaps(d_n_out, 4, d_out, bytes))
+    return fail(HZ_E_INVALID, "d_in, d_out and d_n_out must not overlap");
   int device = 0;
   CK(cudaGetDevice(&device));
   uint32_t *base = nullptr;

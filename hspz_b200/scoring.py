@@ -1,21 +1,30 @@
-"""The 8x8 substitution matrix the extension kernels index with the device
-alphabet, and the LASTZ score-set reader.
+"""Scores for the extension kernels: the 8x8 substitution matrix indexed by
+the device alphabet, and a reader for LASTZ score-set files.
 
-Mirrors hspZ ``src/scoring.rs``: ``build_sub_mat`` (``:41-120``) and
-``load_scoring_matrix`` (``:130-248``).  Only the ACGT block comes from a
-scoring file; the soft-mask / N / X / separator rows are always rebuilt from
-the fixed bad (-1000) and fill (-100) scores, and the separator scores
-``-10 * xdrop`` so that no extension crosses a record boundary.
+The matrix follows hspZ ``src/scoring.rs`` (``build_sub_mat``, ``:41-120``):
+the ACGT block is blastz/HOXD70 unless a score file replaces it; the rows and
+columns of soft-masked (L), N, other (X) and separator (E) codes are always
+derived from fixed values and the ``--ambiguous`` mode, never from the file;
+and the separator scores ``-10 * xdrop`` so that no extension crosses a
+record boundary.
+
+The reader accepts the LASTZ score-set format as KegAlign consumes it
+(``src/scoring.rs:122-278``): ``#`` comments, ``key = value`` settings before
+the matrix (``bad_score`` and ``fill_score`` are used, every other LASTZ
+setting is accepted and has no effect here), one line of column symbols,
+then rows that either start with their own symbol or, blastz style, follow
+the column order.  Pairs the file leaves out take ``fill_score``; a
+nucleotide named by ``bad_score`` takes that score in its row or column.
 """
 from __future__ import annotations
 
 import re
-from typing import List, Optional
+from typing import Dict, Iterator, List, Optional, Tuple
 
 from .sequence import E_NT, L_NT, N_NT, NUC, X_NT
 
-BAD = -1000
-FILL = -100
+BAD = -1000   # soft-masked / unusable pairs
+FILL = -100   # pairs with an unknown (X) base
 
 # blastz / HOXD70 (src/scoring.rs:26-31)
 DEFAULT_ACGT = [
@@ -30,187 +39,190 @@ class ScoringError(ValueError):
     pass
 
 
-# Rust's `str::parse::<i32>`: one optional sign, ASCII digits only.
-_INT_RE = re.compile(r"[+-]?[0-9]+")
+# ---------------------------------------------------------------------------
+# The 8x8 matrix
+
+_SIGNED = re.compile(r"[+-]?[0-9]+\Z")
+
+
+def _as_i32(v: int) -> int:
+    """Two's-complement wrap to 32 bits, as the reference's i32 arithmetic."""
+    v &= 0xFFFFFFFF
+    return v - (1 << 32) if v & 0x80000000 else v
+
+
+def _strict_int(text: str) -> Optional[int]:
+    """An i32 written as an optional sign and decimal digits, else None."""
+    if not _SIGNED.match(text):
+        return None
+    v = int(text)
+    return v if -(1 << 31) <= v < (1 << 31) else None
+
+
+def _ambiguity(spec: str) -> Tuple[str, int, int]:
+    """(mode, reward, penalty) of an ``--ambiguous`` value.
+
+    The mode is the text before the first comma.  With exactly three
+    comma-separated parts the other two give the reward for an N/IUPAC code
+    against itself and the (positive) penalty against anything else; the
+    bare modes ``n`` and ``iupac`` score both as 0, and anything else leaves
+    them at -100."""
+    parts = spec.split(",")
+    mode = parts[0]
+    if len(parts) == 3:
+        reward = _strict_int(parts[1])
+        if reward is None:
+            raise ScoringError(f"--ambiguous {spec!r}: the reward {parts[1]!r} is not an integer")
+        penalty = _strict_int(parts[2])
+        if penalty is None:
+            raise ScoringError(f"--ambiguous {spec!r}: the penalty {parts[2]!r} is not an integer")
+        return mode, reward, _as_i32(-penalty)
+    if spec in ("n", "iupac"):
+        return mode, 0, 0
+    return mode, -100, -100
 
 
 def build_sub_mat(ambiguous: str = "", xdrop: int = 910, scoring: Optional[str] = None) -> List[int]:
-    acgt = load_scoring_matrix(scoring) if scoring else [row[:] for row in DEFAULT_ACGT]
-    fields = ambiguous.split(",")
-    field = fields[0]
-    if len(fields) == 3:
-        try:
-            reward = int(fields[1])
-        except ValueError as e:
-            raise ScoringError(f"--ambiguous reward: {e}")
-        try:
-            penalty = -int(fields[2])
-        except ValueError as e:
-            raise ScoringError(f"--ambiguous penalty: {e}")
-    elif ambiguous in ("n", "iupac"):
-        reward, penalty = 0, 0
+    """The row-major 8x8 matrix ``m[ref_code * 8 + query_code]``."""
+    acgt = load_scoring_matrix(scoring) if scoring else [list(r) for r in DEFAULT_ACGT]
+    mode, reward, penalty = _ambiguity(ambiguous)
+    separator = _as_i32(-10 * xdrop)
+    n_scored = mode in ("n", "iupac")
+
+    def pair(r: int, c: int) -> int:
+        # every non-ACGT row and column is symmetric; the higher code decides
+        hi, lo = max(r, c), min(r, c)
+        if hi == E_NT:
+            return separator
+        if hi == X_NT:
+            if mode == "iupac":
+                return reward if lo == X_NT else penalty
+            # X against a nucleotide or itself is a fill; against L or N, bad
+            return FILL if (lo < L_NT or lo == X_NT) else BAD
+        if hi == N_NT:
+            if n_scored:
+                return reward if lo == N_NT else penalty
+            return BAD
+        if hi == L_NT:
+            return BAD
+        return acgt[r][c]
+
+    return [pair(r, c) for r in range(NUC) for c in range(NUC)]
+
+
+# ---------------------------------------------------------------------------
+# LASTZ score-set files
+
+_HEX2 = re.compile(r"\+?[0-9A-Fa-f]{1,2}\Z")
+
+
+def _symbol(tok: str, where: str) -> int:
+    """A matrix symbol: one ASCII character, or its code as two hex digits."""
+    if "~" in tok:
+        raise ScoringError(f"{where}: `{tok}` is a quantum-alphabet symbol; only nucleotide symbols are read")
+    if len(tok) == 1:
+        code = ord(tok)
+    elif len(tok) == 2 and _HEX2.match(tok):
+        code = int(tok, 16)
     else:
-        reward, penalty = -100, -100
-
-    m = [0] * (NUC * NUC)
-    l, n, x, e = L_NT, N_NT, X_NT, E_NT
-    for i in range(l):
-        for j in range(l):
-            m[i * NUC + j] = acgt[i][j]
-    for i in range(l):
-        m[i * NUC + l] = BAD
-        m[l * NUC + i] = BAD
-    m[l * NUC + l] = BAD
-
-    n_score = (penalty, reward) if field in ("n", "iupac") else (BAD, BAD)
-    for i in range(n):
-        m[i * NUC + n] = n_score[0]
-        m[n * NUC + i] = n_score[0]
-    m[n * NUC + n] = n_score[1]
-
-    if field == "iupac":
-        for i in range(x):
-            m[i * NUC + x] = penalty
-            m[x * NUC + i] = penalty
-        m[x * NUC + x] = reward
-    else:
-        for i in range(l):
-            m[i * NUC + x] = FILL
-            m[x * NUC + i] = FILL
-        for i in range(l, x):
-            m[i * NUC + x] = BAD
-            m[x * NUC + i] = BAD
-        m[x * NUC + x] = FILL
-
-    sep = _wrap_i32(-10 * xdrop)
-    for i in range(e):
-        m[i * NUC + e] = sep
-        m[e * NUC + i] = sep
-    m[e * NUC + e] = sep
-    return m
-
-
-def _wrap_i32(v: int) -> int:
-    v &= 0xFFFFFFFF
-    return v - (1 << 32) if v >= 1 << 31 else v
-
-
-def _parse_char_code(field: str, at: str) -> Optional[int]:
-    if not field:
-        return None
-    if "~" in field:
-        raise ScoringError(
-            f"quantum alphabet column `{field}` is not supported ({at}); only the ACGT block is used")
-    if len(field) == 1:
-        code = ord(field)
-    elif len(field) == 2:
-        try:
-            code = int(field, 16)
-        except ValueError:
-            raise ScoringError(f"invalid character code `{field}` ({at})")
-    else:
-        raise ScoringError(f"invalid character code `{field}` ({at})")
-    if code == 0 or code >= 128:
-        raise ScoringError(f"character code `{field}` out of range ({at})")
+        raise ScoringError(f"{where}: `{tok}` is neither one character nor two hex digits")
+    if not 0 < code < 128:
+        raise ScoringError(f"{where}: symbol `{tok}` is not a printable ASCII code")
     return code
 
 
-def _parse_score(field: str, at: str) -> int:
-    try:
-        if not _INT_RE.fullmatch(field):
-            raise ValueError
-        v = int(field)
-        if not -(1 << 31) <= v < (1 << 31):
-            raise ValueError
-        return v
-    except ValueError:
-        raise ScoringError(f"invalid score `{field}` ({at}); scores must be integers")
+def _score(tok: str, where: str) -> int:
+    v = _strict_int(tok)
+    if v is None:
+        raise ScoringError(f"{where}: `{tok}` is not an integer score")
+    return v
+
+
+def _content(text: str) -> Iterator[Tuple[int, str]]:
+    """(line number, text) of every line that still has text once its
+    ``#`` comment and surrounding blanks are gone."""
+    for no, raw in enumerate(text.splitlines(), start=1):
+        body = raw.partition("#")[0].strip()
+        if body:
+            yield no, body
+
+
+class _Settings:
+    def __init__(self):
+        self.bad = BAD
+        self.fill = FILL
+        self.bad_row: Optional[int] = None
+        self.bad_col: Optional[int] = None
+
+    def apply(self, key: str, value: str, where: str) -> None:
+        if key == "fill_score":
+            self.fill = _score(value, where)
+        elif key == "bad_score":
+            # `score`, `symbol:score` (row and column) or `row:column:score`
+            spec = value.split(":")
+            if len(spec) > 3:
+                raise ScoringError(f"{where}: bad_score takes score, symbol:score or row:column:score")
+            self.bad = _score(spec[-1], where)
+            if len(spec) >= 2:
+                self.bad_row = _symbol(spec[0], where) if spec[0] else None
+                self.bad_col = self.bad_row
+            if len(spec) == 3:
+                self.bad_col = _symbol(spec[1], where) if spec[1] else None
+        # gap penalties, thresholds and the like do not reach the ACGT block
 
 
 def load_scoring_matrix(path: str) -> List[List[int]]:
-    """ACGT block of a LASTZ score-set file (src/scoring.rs:130-248)."""
+    """The 4x4 ACGT block of a LASTZ score-set file."""
     with open(path, "r") as fh:
-        text = fh.read()
-    lines = []
-    for i, raw in enumerate(text.splitlines()):
-        l = raw.split("#", 1)[0].strip()
-        if l:
-            lines.append((i + 1, l))
-    at = lambda n: f"{path}: line {n}"
+        lines = list(_content(fh.read()))
 
-    bad_score, fill_score = BAD, FILL
-    bad_row = bad_col = None
-    header = None
-    idx = 0
-    while idx < len(lines):
-        n, line = lines[idx]
-        idx += 1
-        if "=" not in line:
-            header = (n, line)
-            break
-        key, value = line.split("=", 1)
-        key, value = key.strip(), value.strip()
-        if key == "bad_score":
-            parts = value.split(":")
-            bad_score = _parse_score(parts[-1], at(n))
-            if len(parts) == 1:
-                pass
-            elif len(parts) == 2:
-                bad_row = _parse_char_code(parts[0], at(n))
-                bad_col = bad_row
-            elif len(parts) == 3:
-                bad_row = _parse_char_code(parts[0], at(n))
-                bad_col = _parse_char_code(parts[1], at(n))
-            else:
-                raise ScoringError(f"malformed bad_score ({at(n)})")
-        elif key == "fill_score":
-            fill_score = _parse_score(value, at(n))
-    if header is None:
-        raise ScoringError(f"{path}: no scoring matrix")
-    hn, hline = header
-    col_chars = []
-    for f in hline.split():
-        c = _parse_char_code(f, at(hn))
-        if c is None:
-            raise ScoringError(f"empty column label ({at(hn)})")
-        col_chars.append(c)
-    num_cols = len(col_chars)
-    if num_cols == 0:
-        raise ScoringError(f"{path}: no score columns")
+    def where(no: int) -> str:
+        return f"{path}, line {no}"
 
-    sub = {}
-    num_fields = None
-    implicit_row = 0
-    for n, line in lines[idx:]:
-        fields = line.split()
-        if num_fields is None:
-            if len(fields) not in (num_cols, num_cols + 1):
-                raise ScoringError(
-                    f"wrong number of score columns: got {len(fields)}, expected {num_cols} or "
-                    f"{num_cols + 1} ({at(n)})")
-            num_fields = len(fields)
-        elif num_fields != len(fields):
-            raise ScoringError(f"inconsistent number of score columns ({at(n)})")
-        if len(fields) == num_cols:
-            if implicit_row >= num_cols:
-                raise ScoringError(f"too many score rows ({at(n)})")
-            implicit_row += 1
-            row_char, values = col_chars[implicit_row - 1], fields
+    settings = _Settings()
+    k = 0
+    while k < len(lines) and "=" in lines[k][1]:
+        no, body = lines[k]
+        key, _, value = body.partition("=")
+        settings.apply(key.strip(), value.strip(), where(no))
+        k += 1
+    if k == len(lines):
+        raise ScoringError(f"{path}: no matrix header line (column symbols) after the settings")
+    header_no, header = lines[k]
+    columns = [_symbol(tok, where(header_no)) for tok in header.split()]
+
+    scores: Dict[Tuple[int, int], int] = {}
+    width = None  # fields per row, fixed by the first row
+    unlabelled = 0
+    for no, body in lines[k + 1:]:
+        toks = body.split()
+        if width is None:
+            if len(toks) not in (len(columns), len(columns) + 1):
+                raise ScoringError(f"{where(no)}: a matrix row holds {len(columns)} scores, optionally after "
+                                   f"its symbol; this one has {len(toks)} fields")
+            width = len(toks)
+        elif len(toks) != width:
+            raise ScoringError(f"{where(no)}: {len(toks)} fields where the rows above have {width}")
+        if width == len(columns):
+            if unlabelled == len(columns):
+                raise ScoringError(f"{where(no)}: more unlabelled rows than column symbols")
+            row = columns[unlabelled]
+            unlabelled += 1
         else:
-            row_char = _parse_char_code(fields[0], at(n))
-            if row_char is None:
-                raise ScoringError(f"invalid row character code ({at(n)})")
-            values = fields[1:]
-        for ix, v in enumerate(values):
-            sub[(row_char, col_chars[ix])] = _parse_score(v, at(n))
-    if num_fields is None:
-        raise ScoringError(f"{path}: contains no score rows")
+            row = _symbol(toks[0], where(no))
+            toks = toks[1:]
+        for col, tok in zip(columns, toks):
+            scores[(row, col)] = _score(tok, where(no))
+    if width is None:
+        raise ScoringError(f"{path}: the matrix has column symbols but no rows")
 
-    out = [[0] * 4 for _ in range(4)]
-    for xi, r in enumerate(b"ACGT"):
-        for yi, c in enumerate(b"ACGT"):
-            if bad_row == r or bad_col == c:
-                out[xi][yi] = bad_score
+    block = []
+    for r in b"ACGT":
+        out_row = []
+        for c in b"ACGT":
+            if r == settings.bad_row or c == settings.bad_col:
+                out_row.append(settings.bad)
             else:
-                out[xi][yi] = sub.get((r, c), fill_score)
-    return out
+                out_row.append(scores.get((r, c), settings.fill))
+        block.append(out_row)
+    return block

@@ -201,12 +201,17 @@ int hz_dedup_and_order(hz_segment_pair *h, uint64_t n, uint64_t *n_out);
  *   d_out:   room for n records; receives the kept records in LASTZ order.
  *   d_n_out: one device uint32, receives the kept count.
  *   stream:  a cudaStream_t (NULL for the default stream).
+ * d_in, d_out and d_n_out must not overlap (no in-place dedup); overlapping
+ * buffers are refused with HZ_E_INVALID.
  * The work is queued on `stream` and the call returns at once; results are
- * valid once the stream reaches that point.  The first call on a device
- * looks up the scratch array's device address, so make it before any stream
- * capture.  All calls share the one scratch array: calls whose work overlaps
- * on the GPU (other streams, other host threads) race and corrupt each
- * other's results, so keep them ordered on one stream. */
+ * valid once the stream reaches that point.  The first call in a device's
+ * context looks up the scratch array's device address, so make it before
+ * any stream capture; a process that resets the device (cudaDeviceReset)
+ * gets a new context, and its next call looks the address up again, so that
+ * call too belongs outside a capture.  All calls share the one scratch
+ * array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race and corrupt each other's results, so keep them ordered on
+ * one stream. */
 #define HZ_NOALLOC_MAX_HSPS (1u << 18)
 int hz_dedup_and_order_device_noalloc(const hz_segment_pair *d_in, uint32_t n, hz_segment_pair *d_out,
                                       uint32_t *d_n_out, void *stream);

@@ -1,7 +1,7 @@
 """Regenerates tests/golden/fixtures/ from the reference's own fixture
 generator (hspZ assets/tests/gen_fixtures.py, deterministic seed 20260811).
 
-Run in a checkout that has the reference next to it:
+Run with the root of an hspZ checkout, as an argument or in HSPZ_REFERENCE:
     python tests/golden/make_fixtures.py /path/to/hspZ
 The FASTA files it writes are committed, so nothing at test time needs the
 reference.  expected.json records, per fixture, the HSP count, file count and
@@ -47,4 +47,7 @@ def write_expected():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HSPZ_REFERENCE")
+    if not root:
+        raise SystemExit("usage: make_fixtures.py <hspZ checkout> (or set HSPZ_REFERENCE)")
+    main(root)

@@ -34,12 +34,12 @@ def test_undefined_pairs_take_fill(tmp_path):
 
 
 @pytest.mark.parametrize("body,want", [
-    ("  A  C\nA 1 2\nC 3\n", "inconsistent number of score columns"),
-    ("  A  C\nA 1 2 3 4\n", "wrong number of score columns"),
-    ("  A\nA 1.5\n", "scores must be integers"),
-    ("  A~T\nA 1\n", "quantum alphabet"),
-    ("fill_score = -1\n", "no scoring matrix"),
-    ("  A  C\n", "contains no score rows"),
+    ("  A  C\nA 1 2\nC 3\n", "where the rows above have 3"),
+    ("  A  C\nA 1 2 3 4\n", "holds 2 scores, optionally after its symbol"),
+    ("  A\nA 1.5\n", "is not an integer score"),
+    ("  A~T\nA 1\n", "quantum-alphabet symbol"),
+    ("fill_score = -1\n", "no matrix header line"),
+    ("  A  C\n", "column symbols but no rows"),
 ])
 def test_rejects_malformed(tmp_path, body, want):
     with pytest.raises(ScoringError, match=want):

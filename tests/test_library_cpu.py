@@ -82,3 +82,26 @@ def test_library_dedup_matches_oracle():
     # wrapping diagonal: query start beyond ref start sorts last (src/hsp.rs:298-303)
     a = np.array([(4, 10, 0, 0), (10, 4, 0, 0)], dtype=oracle.HSP_DTYPE)
     assert E.dedup_and_order(a).tolist() == [(10, 4, 0, 0), (4, 10, 0, 0)]
+
+
+def test_noalloc_dedup_refuses_bad_buffers_before_touching_a_device():
+    """The allocation-free dedup checks its arguments on the host first, so
+    these refusals need no GPU: too many records, null, misaligned and
+    overlapping buffers (it reads d_in while writing d_out, so an in-place
+    call would corrupt its own input)."""
+    lib = N.lib()
+    f = lib.hz_dedup_and_order_device_noalloc
+    P = C.c_void_p
+    n = 1000
+    cases = [
+        ((1 << 18) + 1, P(0x100000), P(0x900000), P(0x80), "fixed scratch"),
+        (n, None, P(0x900000), P(0x80), "null device pointer"),
+        (n, P(0x100002), P(0x900000), P(0x80), "4-byte aligned"),
+        (n, P(0x100000), P(0x100000), P(0x80), "must not overlap"),            # in place
+        (n, P(0x100000), P(0x100000 + 16 * n - 16), P(0x80), "must not overlap"),  # last record shared
+        (n, P(0x100000), P(0x900000), P(0x100000 + 64), "must not overlap"),   # count inside d_in
+        (n, P(0x100000), P(0x900000), P(0x900000 + 16 * n - 4), "must not overlap"),  # count inside d_out
+    ]
+    for count, d_in, d_out, d_n, msg in cases:
+        assert f(d_in, count, d_out, d_n, None) == N.HZ_E_INVALID
+        assert msg.encode() in lib.hz_last_error()
