@@ -1432,16 +1432,30 @@ int run_pass_multi(hz_engine *e, int k, const std::vector<HostCall> &calls, std:
   std::vector<std::vector<WaveRecord>> per(calls.size());
   std::atomic<size_t> next{0};
   std::atomic<bool> stop{false};
-  auto drive = [&](hz_engine *x, hz_stats *sx) -> int {
+  // calls an extra workspace could not finish for lack of device memory;
+  // this engine runs them once the others are done
+  std::vector<size_t> orphans;
+  std::mutex orphans_mu;
+  auto drive = [&](hz_engine *x, hz_stats *sx, bool extra) -> int {
     for (;;) {
       if (stop.load()) return HZ_OK;
       size_t i = next.fetch_add(1);
       if (i >= calls.size()) return HZ_OK;
-      int rc = run_wave(x, &calls[i], 1, nullptr, x->cfg.transitions, &per[i], sx, false, false, nullptr, (uint32_t)i);
+      hz_stats one;  // counted only once the call has finished
+      memset(&one, 0, sizeof one);
+      int rc = run_wave(x, &calls[i], 1, nullptr, x->cfg.transitions, &per[i], &one, false, false, nullptr,
+                        (uint32_t)i);
+      if (rc == HZ_E_OOM && extra) {  // this workspace stops; its call moves on
+        per[i].clear();
+        std::lock_guard<std::mutex> lock(orphans_mu);
+        orphans.push_back(i);
+        return HZ_E_OOM;
+      }
       if (rc != HZ_OK) {
         stop.store(true);
         return rc;
       }
+      add_stats(sx, one);
     }
   };
   std::vector<hz_stats> sts(ws.size());
@@ -1458,18 +1472,26 @@ int run_pass_multi(hz_engine *e, int k, const std::vector<HostCall> &calls, std:
           stop.store(true);
           return;
         }
-        rcs[j] = drive(ws[j], &sts[j]);
+        rcs[j] = drive(ws[j], &sts[j], true);
         if (rcs[j] != HZ_OK) errs[j] = g_err;
       });
-    } catch (const std::exception &ex) {  // no thread: its workspace takes no calls
-      rcs[j] = HZ_E_OOM;
-      errs[j] = std::string("plain workspace thread: ") + ex.what();
-      stop.store(true);
+    } catch (const std::exception &) {  // no thread: its workspace takes no calls, the others take them all
       break;
     }
   }
-  rcs[0] = drive(e, &sts[0]);
+  rcs[0] = drive(e, &sts[0], false);
   for (auto &t : helpers) t.join();
+  if (rcs[0] == HZ_OK && !stop.load()) {
+    std::sort(orphans.begin(), orphans.end());
+    for (size_t i : orphans) {
+      hz_stats one;
+      memset(&one, 0, sizeof one);
+      rcs[0] = run_wave(e, &calls[i], 1, nullptr, e->cfg.transitions, &per[i], &one, false, false, nullptr,
+                        (uint32_t)i);
+      if (rcs[0] != HZ_OK) break;
+      add_stats(&sts[0], one);
+    }
+  }
   // the extra workspaces' kernels and profiles count as this engine's
   for (size_t j = 1; j < ws.size(); j++) {
     hz_engine *w = ws[j];
@@ -1482,9 +1504,18 @@ int run_pass_multi(hz_engine *e, int k, const std::vector<HostCall> &calls, std:
     w->prof.clear();
     w->prof_order.clear();
   }
+  // a workspace that ran out of device memory gives back what it holds (it
+  // is made again on a later pass)
+  for (size_t j = ws.size() - 1; j >= 1; j--)
+    if (rcs[j] == HZ_E_OOM) {
+      auto it = std::find(e->twins.begin(), e->twins.end(), ws[j]);
+      if (it != e->twins.end()) e->twins.erase(it);
+      hz_engine_destroy(ws[j]);
+      cudaGetLastError();
+    }
   if (rcs[0] != HZ_OK) return rcs[0];
   for (size_t j = 1; j < ws.size(); j++)
-    if (rcs[j] != HZ_OK) return fail(rcs[j], "%s", errs[j].c_str());
+    if (rcs[j] != HZ_OK && rcs[j] != HZ_E_OOM) return fail(rcs[j], "%s", errs[j].c_str());
   for (const hz_stats &x : sts) add_stats(st, x);
   size_t total = 0;
   for (auto &v : per) total += v.size();
@@ -1902,6 +1933,11 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   } else if (k == "plain_streams") {
     if (value < 1 || value > 4) return fail(HZ_E_INVALID, "plain_streams must be 1..4");
     e->plain_streams = (int)value;
+    // workspaces beyond the new count give their wave buffers back
+    while ((int)e->twins.size() > e->plain_streams - 1) {
+      hz_engine_destroy(e->twins.back());
+      e->twins.pop_back();
+    }
   } else if (k == "tile_cap" || k == "cand_cap" || k == "raw_cap") {
     // starting capacities; a wave that needs more grows them and runs again
     if (value < 16 || value > 0x7FFFFFFFll) return fail(HZ_E_INVALID, "%s must be 16..2^31-1", key);
@@ -2090,6 +2126,11 @@ void share_target(hz_engine *w, const hz_engine *e) {
   w->device_dedup = e->device_dedup;
   w->device_dedup_min = e->device_dedup_min;
   w->use_graph = e->use_graph;
+  // starting capacities: at least the owner's (its hints and what its waves
+  // have grown to), keeping what the workspace has grown to itself
+  w->tile_cap = std::max(w->tile_cap, e->tile_cap);
+  w->cand_cap = std::max(w->cand_cap, e->cand_cap);
+  w->raw_cap = std::max(w->raw_cap, e->raw_cap);
 }
 
 // A workspace that shares `e`'s resident target tables without owning them.

@@ -239,10 +239,16 @@ int hz_engine_profile_reset(hz_engine *e);
  * with its own host thread and stream, so one call's read-back and host dedup
  * overlap other calls' kernels; 1: one call at a time on this engine; an
  * engine given a caller's stream by hz_engine_set_stream runs every call on
- * that stream),
+ * that stream.  Each extra workspace is made on first use and holds its own
+ * grow-only wave buffers -- about as much device memory as the largest call
+ * it has run needs, i.e. up to plain_streams times one engine's wave memory
+ * in all -- until the engine is destroyed or plain_streams is lowered, which
+ * frees the workspaces beyond the new count.  A workspace that runs out of
+ * device memory hands its call to this engine and is freed; the pass goes on),
  * "tile_cap" / "cand_cap" / "raw_cap" (starting capacities of the gate's
  * tile table, the candidate list and the raw-HSP list; a wave that needs more
- * grows them and runs again). */
+ * grows them and runs again; the extra workspaces start from at least this
+ * engine's capacities). */
 int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value);
 
 /* Autotuner (no reference counterpart).  Times the batched form on a
