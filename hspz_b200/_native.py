@@ -115,6 +115,7 @@ SIGNATURES = {
     "hz_serve_submit": (C.c_int, [P, P, U64, PU64]),
     "hz_serve_poll": (C.c_int, [P, U64, C.c_int, C.POINTER(P), PU64, C.POINTER(ServeTimesC)]),
     "hz_serve_stats": (C.c_int, [P, C.POINTER(StatsC), PU64, PU64]),
+    "hz_serve_estimate": (C.c_int, [P, C.c_uint64, PU64]),
     "hz_serve_cancel": (C.c_int, [P, U64]),
     "hz_serve_stop": (C.c_int, [P]),
 }

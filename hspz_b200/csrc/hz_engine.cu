@@ -358,6 +358,7 @@ struct hz_engine {
   std::map<std::string, ProfEntry> prof;
   std::vector<std::string> prof_order;
   uint64_t launches = 0;
+  uint64_t cand_seen = 0;  // gate candidates of every finished wave (serving admission learns from it)
 
   cudaEvent_t get_event() {
     if (!event_pool.empty()) {
@@ -798,6 +799,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
 
     // per-scope dedup on the host, in scope order
     uint32_t nraw = t.raw;
+    e->cand_seen += t.cand;
     if (st) {
       st->hits += t.hits;
       st->cells += t.cells;
@@ -2058,7 +2060,6 @@ enum ServeState { kPending = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed
 struct ServeRequest {
   uint64_t ticket = 0;
   std::vector<uint8_t> ascii;
-  uint64_t est_bytes = 0;
   int state = kPending;
   int err = HZ_OK;
   std::string msg;
@@ -2076,7 +2077,19 @@ struct Server {
   std::deque<uint64_t> pending;
   std::unordered_map<uint64_t, std::shared_ptr<ServeRequest>> reqs;
   uint64_t next_ticket = 1;
+  // Device memory against the budget: per worker, the bytes it holds while
+  // idle (its measured buffers) or, while it runs a batch, the larger of
+  // those and the batch's estimate; in_flight is their sum.
   uint64_t budget = 0, in_flight = 0;
+  std::vector<uint64_t> reserved;
+  // rates the estimates use: hits per seed position, candidates and raw HSPs
+  // per hit -- the largest seen so far, starting from the target's average
+  // and 1e-3
+  double hits_per_pos = 0, cand_per_hit = 1e-3, raw_per_hit = 1e-3;
+  int gate_tile = 128;
+  // bumped by a worker whose head request cannot fit while nothing runs:
+  // idle workers then give their buffers back
+  uint64_t trim_epoch = 0;
   uint32_t max_batch = 64;
   bool stopping = false;
   hz_stats totals{};
@@ -2091,10 +2104,56 @@ uint64_t server_launches(Server *s) {
 
 namespace {
 
-// Device working memory a request needs while it runs: both strands of the
-// query store, per-position counts and compaction, and a margin for the
-// candidate, HSP and dedup buffers.
-uint64_t serve_estimate(uint64_t len) { return 2 * len * (1 + 4 + 12) + (1ull << 20); }
+template <typename T> uint64_t dbytes(const DBuf<T> &b) { return b.p ? b.cap * sizeof(T) + 64 : 0; }
+
+// Device bytes an engine's own working buffers hold: its query store (unless
+// it borrows another engine's) and every wave and dedup buffer.
+uint64_t wave_footprint(const hz_engine *w) {
+  uint64_t b = w->aliases_query ? 0 : dbytes(w->qstore.buf);
+  b += dbytes(w->qascii) + dbytes(w->calls) + dbytes(w->pos_hits) + dbytes(w->np_pos) + dbytes(w->call_nz_lo) +
+       dbytes(w->scope_call) + dbytes(w->raw_scope) + dbytes(w->tile_first) + dbytes(w->tile_call) +
+       dbytes(w->np_excl) + dbytes(w->call_hit_lo) + dbytes(w->scope_lo) + dbytes(w->np_partial) +
+       dbytes(w->np_grand) + dbytes(w->tot) + dbytes(w->cand) + dbytes(w->raw) + dbytes(w->d_out);
+  for (const DBuf<uint32_t> *x : {&w->d_perm_a, &w->d_perm_b, &w->d_keys_a, &w->d_keys_b, &w->d_keep,
+                                  &w->d_keep_excl, &w->d_hist, &w->d_hpart, &w->d_total})
+    b += dbytes(*x);
+  return b;
+}
+
+// Gives an idle serving worker's query store, wave and dedup buffers back
+// (they grow again on its next batch, which restages its queries anyway).
+void release_wave_buffers(hz_engine *w) {
+  cudaStreamSynchronize(w->st);
+  if (!w->aliases_query) w->qstore.buf.release();
+  w->qascii.release();
+  for (DBuf<uint32_t> *x : {&w->pos_hits, &w->np_pos, &w->call_nz_lo, &w->scope_call, &w->raw_scope, &w->tile_first,
+                            &w->tile_call, &w->d_perm_a, &w->d_perm_b, &w->d_keys_a, &w->d_keys_b, &w->d_keep,
+                            &w->d_keep_excl, &w->d_hist, &w->d_hpart, &w->d_total})
+    x->release();
+  w->np_excl.release();
+  w->call_hit_lo.release();
+  w->scope_lo.release();
+  w->np_partial.release();
+  w->np_grand.release();
+  w->cand.release();
+  w->raw.release();
+  w->d_out.release();
+  w->calls.release();
+  w->tot.release();
+}
+
+// Device working memory a request of `len` bases is expected to need while
+// it runs: both strands of the query store (1 B per base) and of the
+// per-position counts and compaction (16 B per position), plus the
+// hit-dependent buffers -- the gate's tile table (8 B per tile of hits),
+// candidates (16 B each), raw HSPs (20 B each) and their dedup scratch (24 B
+// each) -- at the server's current rates.
+uint64_t serve_estimate(const Server *s, uint64_t len) {
+  const double pos = 2.0 * (double)len;
+  const double hits = pos * s->hits_per_pos;
+  const double per_hit = 8.0 / s->gate_tile + 16.0 * s->cand_per_hit + 44.0 * s->raw_per_hit;
+  return (uint64_t)(pos * (1 + 16) + hits * per_hit) + (1ull << 20);
+}
 
 // Copies into `w` what a workspace shares with `e`: the resident target
 // tables (borrowed, not owned), the configuration and the launch knobs.
@@ -2161,77 +2220,170 @@ std::shared_ptr<ServeRequest> queued_request(Server *s, uint64_t ticket) {
   return it->second;
 }
 
+// One batched pass of `qs` on worker `w`: the records of request k go to
+// (*out)[k].  Returns the pass's status.
+int serve_pass(hz_engine *w, const std::vector<std::shared_ptr<ServeRequest>> &qs,
+               std::vector<std::vector<hz_pass_record>> *out, hz_stats *st) {
+  std::vector<const uint8_t *> ptrs;
+  std::vector<uint64_t> lens;
+  for (auto &r : qs) {
+    ptrs.push_back(r->ascii.data());
+    lens.push_back(r->ascii.size());
+  }
+  std::vector<HostCall> calls;
+  std::vector<WaveRecord> recs;
+  out->assign(qs.size(), {});
+  TRY(stage_ascii(w, ptrs.data(), lens.data(), (uint32_t)qs.size()));
+  TRY(run_all_staged(w, &calls, &recs, st));
+  for (auto &wr : recs) {
+    const HostCall &c = calls[wr.call];
+    (*out)[c.query].push_back(hz_pass_record{c.interval, c.strand, wr.h});
+  }
+  return HZ_OK;
+}
+
 void serve_worker(Server *s, uint32_t index, hz_engine *w) {
   cudaSetDevice(w->device);
+  uint64_t seen_epoch = 0;
   while (true) {
     std::vector<std::shared_ptr<ServeRequest>> batch;
+    bool trim = false;
     {
       std::unique_lock<std::mutex> lock(s->mu);
       while (true) {
         while (!s->pending.empty() && !queued_request(s, s->pending.front())) s->pending.pop_front();
         if (s->stopping && s->pending.empty()) return;
-        // admit queued requests, in arrival order, while they fit the budget
+        if (s->trim_epoch != seen_epoch) {  // some request waits for idle buffers
+          seen_epoch = s->trim_epoch;
+          if (s->reserved[index]) {
+            trim = true;
+            break;
+          }
+        }
+        // admit queued requests, in arrival order, while this worker's
+        // reservation -- its own buffers or the batch's estimate, whichever
+        // is larger -- fits the budget beside every other worker's
+        const uint64_t others = s->in_flight - s->reserved[index];
+        uint64_t want = 0;
         while (!s->pending.empty() && batch.size() < s->max_batch) {
           auto r = queued_request(s, s->pending.front());
           if (!r) {
             s->pending.pop_front();
             continue;
           }
-          if (s->in_flight + r->est_bytes > s->budget) break;
+          const uint64_t est = serve_estimate(s, r->ascii.size());
+          // (a request alone on an otherwise empty device always runs: its
+          // estimate may have outgrown the budget since it was submitted)
+          const bool alone = batch.empty() && others == 0;
+          if (!alone && others + std::max(s->reserved[index], want + est) > s->budget) break;
           s->pending.pop_front();
           r->state = kRunning;
           r->t_admit = std::chrono::steady_clock::now();
-          s->in_flight += r->est_bytes;
+          want += est;
           s->running += 1;
           batch.push_back(r);
         }
-        if (!batch.empty()) break;
+        if (!batch.empty()) {
+          const uint64_t res = std::max(s->reserved[index], want);
+          s->in_flight += res - s->reserved[index];
+          s->reserved[index] = res;
+          break;
+        }
+        if (!s->pending.empty()) {
+          if (s->reserved[index]) {  // the head does not fit: first give back this worker's own buffers
+            trim = true;
+            break;
+          }
+          if (s->running == 0) {  // nothing will finish: ask the idle workers for theirs
+            s->trim_epoch++;
+            seen_epoch = s->trim_epoch;
+            s->cv_work.notify_all();
+          }
+        }
         s->cv_work.wait(lock);
       }
     }
-    // one batched pass over the admitted queries
-    std::vector<const uint8_t *> ptrs;
-    std::vector<uint64_t> lens;
-    for (auto &r : batch) {
-      ptrs.push_back(r->ascii.data());
-      lens.push_back(r->ascii.size());
+    if (trim) {
+      release_wave_buffers(w);
+      {
+        std::lock_guard<std::mutex> lock(s->mu);
+        const uint64_t fp = wave_footprint(w);
+        s->in_flight = s->in_flight - s->reserved[index] + fp;
+        s->reserved[index] = fp;
+      }
+      s->cv_work.notify_all();
+      continue;
     }
-    std::vector<HostCall> calls;
-    std::vector<WaveRecord> recs;
+    // one batched pass over the admitted queries; if it fails, each request
+    // runs again alone, so only the ones that fail by themselves report it
+    std::vector<std::vector<hz_pass_record>> recs;
+    std::vector<int> rcs(batch.size(), HZ_OK);
+    std::vector<std::string> msgs(batch.size());
     hz_stats st{};
-    uint64_t l0 = w->launches;
-    int rc = stage_ascii(w, ptrs.data(), lens.data(), (uint32_t)batch.size());
-    if (rc == HZ_OK) rc = run_all_staged(w, &calls, &recs, &st);
-    std::string msg = rc == HZ_OK ? std::string() : g_err;
+    uint64_t l0 = w->launches, c0 = w->cand_seen;
+    int rc = serve_pass(w, batch, &recs, &st);
+    if (rc != HZ_OK && batch.size() > 1) {
+      st = hz_stats{};
+      c0 = w->cand_seen;
+      recs.assign(batch.size(), {});
+      for (size_t k = 0; k < batch.size(); k++) {
+        std::vector<std::vector<hz_pass_record>> one;
+        hz_stats s1{};
+        rcs[k] = serve_pass(w, {batch[k]}, &one, &s1);
+        if (rcs[k] == HZ_OK) {
+          recs[k] = std::move(one[0]);
+          add_stats(&st, s1);
+        } else {
+          msgs[k] = g_err;
+        }
+      }
+    } else if (rc != HZ_OK) {
+      rcs[0] = rc;
+      msgs[0] = g_err;
+    }
+    const uint64_t fp = wave_footprint(w);
+    bool over = false;
     {
       std::lock_guard<std::mutex> lock(s->mu);
       auto now = std::chrono::steady_clock::now();
-      if (rc == HZ_OK)
-        for (auto &wr : recs) {
-          const HostCall &c = calls[wr.call];
-          batch[c.query]->recs.push_back(hz_pass_record{c.interval, c.strand, wr.h});
-        }
-      for (auto &r : batch) {
-        r->state = rc == HZ_OK ? kDone : kFailed;
-        r->err = rc;
-        r->msg = msg;
+      uint64_t positions = 0;
+      for (size_t k = 0; k < batch.size(); k++) {
+        auto &r = batch[k];
+        if (rcs[k] == HZ_OK) positions += 2 * r->ascii.size();
+        r->recs = std::move(recs[k]);
+        r->state = rcs[k] == HZ_OK ? kDone : kFailed;
+        r->err = rcs[k];
+        r->msg = msgs[k];
         r->batch_queries = (uint32_t)batch.size();
         r->worker = index;
         r->t_done = now;
         r->ascii.clear();
         r->ascii.shrink_to_fit();
-        s->in_flight -= r->est_bytes;
         s->running -= 1;
       }
-      s->launches += w->launches - l0;
-      if (rc == HZ_OK) {
-        s->totals.seeds += st.seeds;
-        s->totals.hits += st.hits;
-        s->totals.raw_hsps += st.raw_hsps;
-        s->totals.hsps += st.hsps;
-        s->totals.cells += st.cells;
-        s->totals.calls += st.calls;
+      // what this worker holds now replaces the batch's reservation
+      s->in_flight = s->in_flight - s->reserved[index] + fp;
+      s->reserved[index] = fp;
+      over = s->in_flight > s->budget;
+      if (positions && st.hits) {
+        s->hits_per_pos = std::max(s->hits_per_pos, (double)st.hits / (double)positions);
+        s->cand_per_hit = std::max(s->cand_per_hit, (double)(w->cand_seen - c0) / (double)st.hits);
+        s->raw_per_hit = std::max(s->raw_per_hit, (double)st.raw_hsps / (double)st.hits);
       }
+      s->launches += w->launches - l0;
+      s->totals.seeds += st.seeds;
+      s->totals.hits += st.hits;
+      s->totals.raw_hsps += st.raw_hsps;
+      s->totals.hsps += st.hsps;
+      s->totals.cells += st.cells;
+      s->totals.calls += st.calls;
+    }
+    if (over) {  // the batch outgrew its estimate: give the buffers back now
+      release_wave_buffers(w);
+      std::lock_guard<std::mutex> lock(s->mu);
+      const uint64_t left = wave_footprint(w);
+      s->in_flight = s->in_flight - s->reserved[index] + left;
+      s->reserved[index] = left;
     }
     s->cv_done.notify_all();
     s->cv_work.notify_all();
@@ -2264,6 +2416,15 @@ int hz_serve_start(hz_engine *e, const hz_serve_config *cfg) {
     }
     s->workers.push_back(w);
   }
+  s->reserved.assign(s->workers.size(), 0);
+  for (size_t i = 0; i < s->workers.size(); i++) {
+    s->reserved[i] = wave_footprint(s->workers[i]);
+    s->in_flight += s->reserved[i];
+  }
+  // starting rate: a query k-mer drawn uniformly meets per_pos buckets of the
+  // average size
+  s->hits_per_pos = e->index_len ? (double)e->per_pos(e->cfg.transitions) * (double)e->n_pos / (double)e->index_len : 0;
+  s->gate_tile = e->gate_tile;
   e->server = s;
   for (uint32_t i = 0; i < (uint32_t)s->workers.size(); i++) s->threads.emplace_back(serve_worker, s, i, s->workers[i]);
   return HZ_OK;
@@ -2275,15 +2436,15 @@ int hz_serve_submit(hz_engine *e, const uint8_t *ascii, uint64_t len, uint64_t *
   if (!s) return fail(HZ_E_STATE, "the serving loop is not running");
   if (len > 0xFFFFFFFFull) return fail(HZ_E_INVALID, "query block exceeds u32 coordinates");
   auto r = std::make_shared<ServeRequest>();
-  r->est_bytes = serve_estimate(len);
-  if (r->est_bytes > s->budget)
-    return fail(HZ_E_BUDGET, "a %llu-base query needs ~%llu bytes of working memory, above the %llu-byte budget",
-                (unsigned long long)len, (unsigned long long)r->est_bytes, (unsigned long long)s->budget);
-  r->ascii.assign(ascii, ascii + len);
   r->t_submit = std::chrono::steady_clock::now();
   {
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stopping) return fail(HZ_E_STATE, "the serving loop is stopping");
+    const uint64_t est = serve_estimate(s, len);
+    if (est > s->budget)
+      return fail(HZ_E_BUDGET, "a %llu-base query needs ~%llu bytes of working memory, above the %llu-byte budget",
+                  (unsigned long long)len, (unsigned long long)est, (unsigned long long)s->budget);
+    r->ascii.assign(ascii, ascii + len);
     r->ticket = s->next_ticket++;
     s->reqs[r->ticket] = r;
     s->pending.push_back(r->ticket);
@@ -2330,6 +2491,15 @@ int hz_serve_poll(hz_engine *e, uint64_t ticket, int timeout_ms, hz_pass_record 
     memcpy(*out, r->recs.data(), r->recs.size() * sizeof(hz_pass_record));
   }
   *n = r->recs.size();
+  return HZ_OK;
+}
+
+int hz_serve_estimate(hz_engine *e, uint64_t len, uint64_t *bytes) {
+  if (!e || !bytes) return fail(HZ_E_INVALID, "null argument");
+  Server *s = e->server;
+  if (!s) return fail(HZ_E_STATE, "the serving loop is not running");
+  std::lock_guard<std::mutex> lock(s->mu);
+  *bytes = serve_estimate(s, len);
   return HZ_OK;
 }
 

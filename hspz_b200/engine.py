@@ -246,6 +246,13 @@ class Engine:
                                       C.byref(tm)))
         return _take(out, n.value, PASS_RECORD), tm.as_dict()
 
+    def serve_estimate(self, length: int) -> int:
+        """Device working memory the serving loop expects a request of
+        `length` bases to need now."""
+        b = C.c_uint64()
+        N.check(N.lib().hz_serve_estimate(self._h, int(length), C.byref(b)))
+        return b.value
+
     def serve_stats(self):
         """(totals over finished batches, requests queued, requests running)."""
         st, q, r = N.StatsC(), C.c_uint64(), C.c_uint64()

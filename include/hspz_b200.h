@@ -285,11 +285,23 @@ int hz_engine_set_stream(hz_engine *e, void *stream);
  * target resident and take query blocks as they arrive.  hz_serve_start
  * starts `workers` host threads, each with its own query store, wave buffers
  * and stream over the engine's target tables.  A free worker takes the queued
- * requests in arrival order while their estimated device working memory fits
- * under `budget_bytes` (at most `max_batch_queries` of them, 0 = 64) and runs
- * them as one batched pass, so requests that arrive while others run join the
- * next batch.  A request's records equal what hz_run_pass returns for that
- * query block alone. */
+ * requests in arrival order (at most `max_batch_queries` of them, 0 = 64) and
+ * runs them as one batched pass, so requests that arrive while others run
+ * join the next batch.  A request's records equal what hz_run_pass returns
+ * for that query block alone.
+ * Admission by memory: every worker holds device memory -- its grow-only
+ * query store, wave and dedup buffers -- and counts against `budget_bytes`
+ * with what it measurably holds while idle, or, while it runs a batch, the
+ * larger of that and the batch's estimate (hz_serve_estimate per request).
+ * A batch is formed only while the sum over all workers stays within the
+ * budget.  A worker whose buffers outgrow the budget after a batch frees
+ * them; idle workers free theirs when a queued request could not fit
+ * otherwise.  The estimates grow with the hits per position, candidates and
+ * raw HSPs per hit the loop has seen, so a request accepted by
+ * hz_serve_submit may later estimate above the whole budget; it then runs
+ * alone once no other worker holds memory.
+ * Failures: if a batch fails, each of its requests runs again alone, so only
+ * a request that fails by itself reports an error. */
 typedef struct hz_serve_config {
   uint64_t budget_bytes;       /* device working memory for requests in flight */
   uint32_t workers;            /* 1..8 */
@@ -317,6 +329,9 @@ int hz_serve_submit(hz_engine *e, const uint8_t *ascii, uint64_t len, uint64_t *
  * cancelled one).  HZ_E_INVALID for an unknown or consumed ticket. */
 int hz_serve_poll(hz_engine *e, uint64_t ticket, int timeout_ms, hz_pass_record **out, uint64_t *n,
                   hz_serve_times *times);
+/* The device working memory the loop currently expects a request of `len`
+ * bases to need (the figure admission and hz_serve_submit use). */
+int hz_serve_estimate(hz_engine *e, uint64_t len, uint64_t *bytes);
 /* Totals (seeds, hits, cells, HSPs, calls) over every batch finished since
  * hz_serve_start, and the requests still queued or running. */
 int hz_serve_stats(hz_engine *e, hz_stats *stats, uint64_t *queued, uint64_t *running);

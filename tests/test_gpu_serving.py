@@ -17,11 +17,6 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("interval", "strand", "ref_start", "query_start", "len", "score")
 
 
-def serve_estimate(n: int) -> int:
-    """Working-memory estimate the library admits a request by."""
-    return 2 * n * (1 + 4 + 12) + (1 << 20)
-
-
 @pytest.fixture(scope="module", autouse=True)
 def built():
     build()
@@ -83,7 +78,11 @@ def test_budget_admits_one_request_at_a_time_and_refuses_oversized(workload, alo
             want.append(rows(ref.run_pass()[0]))
     with Engine(EngineConfig()) as e:
         e.load_target(target)
-        e.serve_start(budget_bytes=serve_estimate(n) + 1000, workers=2)
+        e.serve_start(budget_bytes=1 << 40, workers=2)
+        est = e.serve_estimate(n)  # what one request of n bases is expected to need
+        assert e.serve_estimate(2 * n) > est + 1000
+        e.serve_stop()
+        e.serve_start(budget_bytes=est + 1000, workers=2)
         with pytest.raises(N.HzError) as ex:
             e.serve_submit(b"A" * (2 * n))
         assert ex.value.code == N.HZ_E_BUDGET
@@ -160,6 +159,37 @@ def test_failing_request_reports_its_own_error():
         e.serve_stop()
         e.swap_query_ascii(clean)
         assert rows(got) == rows(e.run_pass()[0])
+
+
+def test_a_failing_request_fails_alone_in_its_batch():
+    """A batch holding one request that fails on its own: the batch is rerun
+    request by request, so only that request reports the error and the
+    others return exactly what run_pass gives them alone."""
+    rng = np.random.default_rng(6)
+    rep = synth.random_bases(rng, 2000)
+    target = np.concatenate([synth.random_bases(rng, 50_000), rep, synth.random_bases(rng, 3000), rep,
+                             synth.random_bases(rng, 3000), rep])
+    busy = synth.random_bases(rng, 400_000)
+    good = [synth.random_bases(rng, 30_000), synth.random_bases(rng, 25_000)]
+    with Engine(EngineConfig(max_hits=1)) as e:  # the repeat's first seed holds 3 hits: no valid MAX_HITS cut
+        e.load_target(target)
+        want = []
+        for q in [busy] + good:
+            e.swap_query_ascii(q)
+            want.append(rows(e.run_pass()[0]))
+        e.serve_start(budget_bytes=1 << 30, workers=1, max_batch_queries=8)
+        t_busy = e.serve_submit(busy)  # keeps the one worker while the next three queue
+        t = [e.serve_submit(good[0]), e.serve_submit(rep), e.serve_submit(good[1])]
+        got, _ = e.serve_poll(t_busy)
+        assert rows(got) == want[0]
+        with pytest.raises(N.HzError) as ex:
+            e.serve_poll(t[1])
+        assert ex.value.code == N.HZ_E_INVALID
+        for ticket, w in ((t[0], want[1]), (t[2], want[2])):
+            got, tm = e.serve_poll(ticket)
+            assert rows(got) == w
+            assert tm["batch_queries"] == 3  # it shared a batch with the failing request
+        e.serve_stop()
 
 
 def test_many_workers_random_poll_order_and_totals():
