@@ -227,6 +227,22 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148u * 64u) {
 
 }  // namespace
 
+// A sequence packed 2 bits per base for the lockstep gate (pack2_kernel):
+// the forward half and the reversed half, each `half` bases, codes and
+// special masks.
+struct Packed {
+  DBuf<uint32_t> code2, special;
+  uint64_t half = 0;
+  bool valid = false;
+  const uint32_t *code(int rev) const { return code2.p + (rev ? half / 16 : 0); }
+  const uint32_t *spec(int rev) const { return special.p + (rev ? half / 32 : 0); }
+  void release() {
+    code2.release();
+    special.release();
+    valid = false;
+  }
+};
+
 // ---------------------------------------------------------------------------
 
 // One call as the host sees it: a WGA chunk [start, end) of one strand of one
@@ -302,6 +318,7 @@ struct hz_engine {
         b->release();
     }
   } build;
+  Packed ref_p;  // the reference packed for the lockstep gate
   bool has_target = false;
   bool owns_target = true;         // false for serving workers that share the owner's tables
   bool aliases_query = false;      // true for the plain form's extra workspaces (see run_pass_multi)
@@ -310,6 +327,7 @@ struct hz_engine {
   struct Server *server = nullptr;  // the serving loop, while one runs
   // query store
   SeqBuf qstore;
+  Packed qry_p;  // the query store packed for the lockstep gate
   DBuf<uint8_t> qascii;
   std::vector<StagedQuery> queries;
   uint32_t cur_query = 0;  // the query the per-call entry points work on
@@ -336,6 +354,7 @@ struct hz_engine {
   HBuf<ScopedHspOut> h_out;
   uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
   // tuning
+  int gate_version = 2;  // 2: lockstep gate over packed sequences (when the scores allow), 1: lane-refill gate
   int gate_tile = 128;  // hits per gate warp tile
   uint32_t gate_cap = 128;  // the autotuner's usual choice
   int gate_blocks_per_sm = 0;
@@ -434,6 +453,69 @@ int set_device(hz_engine *e) {
 }
 
 template <int TW> size_t gate_smem() { return sizeof(GateSmem<TW>); }
+
+// Packs n device codes for the lockstep gate (forward and reversed halves).
+int pack_seq(hz_engine *e, const uint8_t *codes, uint64_t n, Packed *p) {
+  cudaStream_t s = e->st;
+  p->valid = false;
+  p->half = (n + 64 + 31) & ~31ull;
+  const uint64_t blocks = 2 * p->half / 32;
+  TRY(p->code2.ensure(2 * blocks + 8, s));
+  TRY(p->special.ensure(blocks + 8, s));
+  CK(cudaMemsetAsync(p->code2.p + 2 * blocks, 0, 8 * sizeof(uint32_t), s));
+  CK(cudaMemsetAsync(p->special.p + blocks, 0, 8 * sizeof(uint32_t), s));
+  uint32_t *c2 = p->code2.p, *sp = p->special.p;
+  const uint64_t half = p->half;
+  TRY(e->launch("pack", [&] { pack2_kernel<<<grid_for(blocks, 256), 256, 0, s>>>(codes, n, half, c2, sp); }));
+  p->valid = true;
+  return HZ_OK;
+}
+
+// The lockstep gate reads each cell's score as a signed byte and keeps
+// positions in 32 bits; otherwise the lane-refill gate runs.
+bool gate2_usable(const hz_engine *e) {
+  if (e->gate_version != 2 || !e->ref_p.valid || !e->qry_p.valid) return false;
+  if ((uint64_t)e->rlen + 128 >= (1ull << 32) || (uint64_t)e->qstore.len + 128 >= (1ull << 32)) return false;
+  for (int r = 0; r < 4; r++)
+    for (int q = 0; q < 4; q++) {
+      const int32_t v = e->cfg.sub_mat[r * kNuc + q];
+      if (v < -128 || v > 127) return false;
+    }
+  return true;
+}
+
+template <int TW> size_t gate2_smem() { return sizeof(Gate2Smem<TW>); }
+
+template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
+  static bool configured[64] = {false};
+  static std::mutex mu;  // serving workers launch from several host threads
+  size_t smem = gate2_smem<TW>();
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!configured[e->device & 63]) {
+      CK(cudaFuncSetAttribute(gate2_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured[e->device & 63] = true;
+    }
+  }
+  int per_sm = e->gate_blocks_per_sm;
+  if (per_sm <= 0) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate2_kernel<TW>, kGateThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  Gate2Args a2;
+  a2.g = ga;
+  a2.ref2 = e->ref_p.code(0);
+  a2.refm = e->ref_p.spec(0);
+  a2.ref2r = e->ref_p.code(1);
+  a2.refmr = e->ref_p.spec(1);
+  a2.qry2 = e->qry_p.code(0);
+  a2.qrym = e->qry_p.spec(0);
+  a2.qry2r = e->qry_p.code(1);
+  a2.qrymr = e->qry_p.spec(1);
+  a2.qtotal = (uint32_t)e->qstore.len;
+  unsigned grid = (unsigned)(e->sm_count * per_sm);
+  return e->launch("gate", [&] { gate2_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(a2); });
+}
 
 template <int TW> int launch_gate(hz_engine *e, const GateArgs &ga) {
   static bool configured[64] = {false};
@@ -729,10 +811,18 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       ga.cand_cap = e->cand_cap;
       ga.tile_first = e->tile_first.p;
       ga.tile_call = e->tile_call.p;
-      switch (e->gate_tile) {
-        case 64: TRY(launch_gate<64>(e, ga)); break;
-        case 256: TRY(launch_gate<256>(e, ga)); break;
-        default: TRY(launch_gate<128>(e, ga)); break;
+      if (gate2_usable(e)) {
+        switch (e->gate_tile) {
+          case 64: TRY(launch_gate2<64>(e, ga)); break;
+          case 256: TRY(launch_gate2<256>(e, ga)); break;
+          default: TRY(launch_gate2<128>(e, ga)); break;
+        }
+      } else {
+        switch (e->gate_tile) {
+          case 64: TRY(launch_gate<64>(e, ga)); break;
+          case 256: TRY(launch_gate<256>(e, ga)); break;
+          default: TRY(launch_gate<128>(e, ga)); break;
+        }
       }
       ExactArgs xa;
       xa.ref = w.ref;
@@ -905,6 +995,7 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
       encode_kernel<<<grid_for(len / 4 + 1, 256), 256, 0, s>>>(e->qascii.p, len, f, r);
     }));
   }
+  TRY(pack_seq(e, e->qstore.base(), total, &e->qry_p));
   TRY(e->sync());
   e->queries = qs;
   e->cur_query = 0;
@@ -1052,8 +1143,12 @@ void hz_engine_destroy(hz_engine *e) {
     e->index_table.release();
     e->pos_table.release();
     e->nbr_hits.release();
+    e->ref_p.release();
   }
-  if (!e->aliases_query) e->qstore.buf.release();
+  if (!e->aliases_query) {
+    e->qstore.buf.release();
+    e->qry_p.release();
+  }
   e->qascii.release();
   e->build.release();
   for (auto &s : e->slot) s.seeds.release();
@@ -1126,6 +1221,7 @@ int hz_engine_load_tables(hz_engine *e, const uint32_t *index_table, uint64_t in
   CK(cudaMemcpyAsync(e->index_table.p, index_table, index_len * 4, cudaMemcpyHostToDevice, s));
   if (pos_len) CK(cudaMemcpyAsync(e->pos_table.p, pos_table, pos_len * 4, cudaMemcpyHostToDevice, s));
   if (ref_len) CK(cudaMemcpyAsync(e->ref.base(), ref_seq, ref_len, cudaMemcpyHostToDevice, s));
+  TRY(pack_seq(e, e->ref.base(), ref_len, &e->ref_p));
   TRY(e->sync());
   TRY(build_nbr_hits(e, index_len));
   e->index_len = index_len;
@@ -1232,6 +1328,7 @@ int hz_engine_load_target(hz_engine *e, const uint8_t *ref_ascii, uint64_t len) 
     TRY(e->sync());
   }
   if (bs.bytes() > kKeepBuildScratch) bs.release();
+  TRY(pack_seq(e, e->ref.base(), len, &e->ref_p));
   TRY(build_nbr_hits(e, index_len));
   e->index_len = index_len;
   e->n_pos = n_valid;
@@ -1269,6 +1366,7 @@ int hz_swap_query(hz_engine *e, const uint8_t *query, const uint8_t *query_rc, u
     CK(cudaMemcpyAsync(e->qstore.base() + q.off_f, query, len, cudaMemcpyHostToDevice, e->st));
     CK(cudaMemcpyAsync(e->qstore.base() + q.off_r, query_rc, len, cudaMemcpyHostToDevice, e->st));
   }
+  TRY(pack_seq(e, e->qstore.base(), total, &e->qry_p));
   TRY(e->sync());
   e->queries.assign(1, q);
   e->cur_query = 0;
@@ -1422,6 +1520,7 @@ int run_pass_multi(hz_engine *e, int k, const std::vector<HostCall> &calls, std:
     w->qstore.buf.p = e->qstore.buf.p;
     w->qstore.buf.cap = e->qstore.buf.cap;
     w->qstore.len = e->qstore.len;
+    w->qry_p = e->qry_p;
     w->queries = e->queries;
     w->cur_query = e->cur_query;
     w->has_query = e->has_query;
@@ -1916,6 +2015,9 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
     if (value != 64 && value != 128 && value != 256)
       return fail(HZ_E_INVALID, "gate_tile must be 64, 128 or 256");
     e->gate_tile = (int)value;
+  } else if (k == "gate_version") {
+    if (value != 1 && value != 2) return fail(HZ_E_INVALID, "gate_version must be 1 or 2");
+    e->gate_version = (int)value;
   } else if (k == "gate_cap") {
     if (value < 8 || value > 65528 || value % 8) return fail(HZ_E_INVALID, "gate_cap must be a multiple of 8 in 8..65528");
     e->gate_cap = (uint32_t)value;
@@ -2109,7 +2211,7 @@ template <typename T> uint64_t dbytes(const DBuf<T> &b) { return b.p ? b.cap * s
 // Device bytes an engine's own working buffers hold: its query store (unless
 // it borrows another engine's) and every wave and dedup buffer.
 uint64_t wave_footprint(const hz_engine *w) {
-  uint64_t b = w->aliases_query ? 0 : dbytes(w->qstore.buf);
+  uint64_t b = w->aliases_query ? 0 : dbytes(w->qstore.buf) + dbytes(w->qry_p.code2) + dbytes(w->qry_p.special);
   b += dbytes(w->qascii) + dbytes(w->calls) + dbytes(w->pos_hits) + dbytes(w->np_pos) + dbytes(w->call_nz_lo) +
        dbytes(w->scope_call) + dbytes(w->raw_scope) + dbytes(w->tile_first) + dbytes(w->tile_call) +
        dbytes(w->np_excl) + dbytes(w->call_hit_lo) + dbytes(w->scope_lo) + dbytes(w->np_partial) +
@@ -2124,7 +2226,10 @@ uint64_t wave_footprint(const hz_engine *w) {
 // (they grow again on its next batch, which restages its queries anyway).
 void release_wave_buffers(hz_engine *w) {
   cudaStreamSynchronize(w->st);
-  if (!w->aliases_query) w->qstore.buf.release();
+  if (!w->aliases_query) {
+    w->qstore.buf.release();
+    w->qry_p.release();
+  }
   w->qascii.release();
   for (DBuf<uint32_t> *x : {&w->pos_hits, &w->np_pos, &w->call_nz_lo, &w->scope_call, &w->raw_scope, &w->tile_first,
                             &w->tile_call, &w->d_perm_a, &w->d_perm_b, &w->d_keys_a, &w->d_keys_b, &w->d_keep,
@@ -2176,8 +2281,10 @@ void share_target(hz_engine *w, const hz_engine *e) {
   w->nbr_hits.cap = e->nbr_hits.cap;
   w->has_nbr = e->has_nbr;
   w->n_pos = e->n_pos;
+  w->ref_p = e->ref_p;
   w->has_target = true;
   w->owns_target = false;
+  w->gate_version = e->gate_version;
   w->gate_tile = e->gate_tile;
   w->gate_cap = e->gate_cap;
   w->gate_blocks_per_sm = e->gate_blocks_per_sm;

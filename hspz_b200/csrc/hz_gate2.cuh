@@ -1,0 +1,395 @@
+// Lockstep score gate over 2-bit packed sequences (included by hz_wave.cuh).
+//
+// The same work as gate_kernel -- fused hit expansion and the X-drop score
+// bound of every hit, src/gpu/kernels.rs:521-1057 -- organised so that a
+// warp's 32 lanes run one instruction stream without divergence in the hot
+// loop:
+//   * a lane owns one hit-direction at a time and scores it in rounds of 32
+//     cells, every lane the same 32 cells' worth of instructions whether its
+//     extension ends in the round or not;
+//   * the reference and query are read 2 bits per base (pack2_kernel), so a
+//     round's cells are two 64-bit windows (five word loads per sequence) and
+//     a cell's substitution score is one byte extract and one shared-memory
+//     byte load from a table indexed by the pair of codes;
+//   * a left extension walks the reversed copy of each sequence forwards, so
+//     both directions are the same code;
+//   * after a round the lanes whose extension ended in it find the exact end
+//     cell and the maximum before it by rescoring one eight-cell group, and
+//     take the next hit-direction from the warp's tile.
+// Bases that are not uppercase ACGT (soft-masked, N, other, separator) are
+// marked in a side mask; a round stops at the first one and that cell is
+// scored from the 8-bit codes and the full 8x8 table.
+//
+// The extension semantics are those of the scalar oracle and the reference
+// warp kernel: S += sub[r][q]; M' = max(M, S) includes the cell; the
+// extension stops at the first cell with M' - S > xdrop and keeps the maximum
+// from before it, or at the edge.  A hit becomes a candidate when
+// (i32)(f32)(right max + left max) >= hspthresh, or when a direction runs
+// past `cap` cells (then the exact kernel redoes it).
+#pragma once
+
+namespace hz {
+
+constexpr int kRound = 32;  // cells a lane scores per round
+
+template <int TW>
+struct WarpTile2 {
+  uint32_t slot_bst[TW];  // pos_table index of the slot's first in-tile hit
+  uint32_t slot_q[TW];    // query anchor (absolute)
+  uint32_t slot_call[TW];
+  uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
+  uint32_t hit_r[TW];     // reference anchor
+  uint32_t hit_q[TW];     // query anchor (absolute)
+  uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
+  uint32_t hit_call[TW];
+};
+
+template <int TW>
+struct Gate2Smem {
+  int32_t sub[64];
+  int8_t tbl[4][256];  // score of the pair of codes a byte of a round's index word holds (see pair_byte)
+  WarpTile2<TW> warp[kGateWarps];
+};
+
+struct Gate2Args {
+  GateArgs g;
+  // packed sequences: codes and special masks of the forward half and of the
+  // reversed half (pack2_kernel)
+  const uint32_t *ref2, *refm, *ref2r, *refmr;
+  const uint32_t *qry2, *qrym, *qry2r, *qrymr;
+  uint32_t qtotal;  // bases of the query store (the reversed query half is it read backwards)
+};
+
+// The four index words of 16 cells: word j holds cells j, j+4, j+8, j+12 in
+// its bytes 0..3, each byte carrying that cell's reference code in bits
+// 2j..2j+1 and its query code in bits 2j+2..2j+3 (j < 3) or 0..1 (j = 3);
+// the other bits are other cells' codes, which tbl[j] ignores.
+__device__ __forceinline__ void pair_words(uint32_t r, uint32_t q, uint32_t t[4]) {
+  const uint32_t q2 = q << 2, q6 = q >> 6;
+  t[0] = (r & 0x03030303u) | (q2 & ~0x03030303u);
+  t[1] = (r & 0x0C0C0C0Cu) | (q2 & ~0x0C0C0C0Cu);
+  t[2] = (r & 0x30303030u) | (q2 & ~0x30303030u);
+  t[3] = (r & 0xC0C0C0C0u) | (q6 & ~0xC0C0C0C0u);
+}
+
+__device__ __forceinline__ void pair_codes(int j, uint32_t b, uint32_t *r, uint32_t *q) {
+  *r = (b >> (2 * j)) & 3u;
+  *q = j < 3 ? (b >> (2 * j + 2)) & 3u : b & 3u;
+}
+
+// Score of cell k (0..15) of the 16 cells whose index words are t.
+__device__ __forceinline__ int32_t cell_score(const int8_t (*tbl)[256], const uint32_t t[4], int k) {
+  return tbl[k & 3][__byte_perm(t[k & 3], 0u, 0x4440u + (uint32_t)(k >> 2))];
+}
+
+__device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+
+// 32 bases of a packed half starting at base p: codes (two words) and specials.
+__device__ __forceinline__ void window32(const uint32_t *code, const uint32_t *spec, uint32_t p, uint32_t *lo,
+                                         uint32_t *hi, uint32_t *sp) {
+  const uint32_t w = p >> 4, sh = (p & 15u) << 1;
+  const uint32_t a0 = __ldg(code + w), a1 = __ldg(code + w + 1), a2 = __ldg(code + w + 2);
+  *lo = __funnelshift_r(a0, a1, sh);
+  *hi = __funnelshift_r(a1, a2, sh);
+  const uint32_t m = p >> 5;
+  *sp = __funnelshift_r(__ldg(spec + m), __ldg(spec + m + 1), p & 31u);
+}
+
+template <int TW>
+__global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
+  static_assert(TW % 32 == 0, "a warp tile is a multiple of 32 hits");
+  const GateArgs &a = a2.g;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Gate2Smem<TW> &sm = *reinterpret_cast<Gate2Smem<TW> *>(smem_raw);
+  if (a.tot->status & 4u) return;  // no tile table: the host reruns the wave with a larger one
+  if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
+  for (uint32_t i = threadIdx.x; i < 1024; i += blockDim.x) {
+    uint32_t r, q;
+    pair_codes((int)(i >> 8), i & 255u, &r, &q);
+    sm.tbl[i >> 8][i & 255u] = (int8_t)a.sub[r * kNuc + q];
+  }
+  __syncthreads();  // the block's only barrier
+  WarpTile2<TW> &wt = sm.warp[threadIdx.x >> 5];
+  const int8_t(*tbl)[256] = sm.tbl;
+  const uint32_t lane = threadIdx.x & 31;
+  const int32_t X = a.xdrop;
+  const uint32_t rlen = a.w.rlen, qtotal = a2.qtotal;
+  unsigned long long cells_acc = 0;
+  const unsigned long long total = a.tot->hits;
+  const uint32_t nz = a.tot->nz;
+  const WaveIn &w = a.w;
+  while (true) {
+    unsigned long long j = 0;
+    if (lane == 0) j = atomicAdd(&a.tot->tiles, 1ull);
+    j = __shfl_sync(0xffffffffu, j, 0);
+    const unsigned long long h0 = j * (unsigned long long)TW;
+    if (h0 >= total) break;
+    const uint32_t nt = (uint32_t)min((unsigned long long)TW, total - h0);
+    // ---- tile setup: the hits' anchors, edge distances and calls ----------
+    const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
+    const uint32_t e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
+    uint32_t c = a.tile_call[j];
+    __syncwarp();  // the previous tile's lanes are done with its arrays
+    for (uint32_t i = lane; i < nt; i += 32) wt.hit_slot[i] = 0;
+    __syncwarp();
+    for (uint32_t k = k0 + lane; k <= e1; k += 32) {
+      uint32_t p = a.np_pos[k];
+      while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+      CallDev cd = w.calls[c];
+      uint32_t qpos, kmer;
+      position_seed(w, cd, p, &qpos, &kmer);
+      unsigned long long lo = a.np_excl[k];
+      const uint32_t q_anchor = cd.qoff + qpos + w.shape.size;
+      for (uint32_t v0 = 0; v0 < w.per_pos; v0 += kLookupBatch) {
+        uint32_t beg[kLookupBatch], cnt[kLookupBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kLookupBatch; u++) {
+          cnt[u] = 0;
+          beg[u] = 0;
+          if (v0 + u < w.per_pos) cnt[u] = bucket(w, seed_variant(kmer, v0 + u), &beg[u]);
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kLookupBatch; u++) {
+          unsigned long long hi = lo + cnt[u];
+          if (cnt[u] && hi > h0 && lo < h0 + nt) {
+            unsigned long long first = lo > h0 ? lo : h0;
+            uint32_t s = (uint32_t)(first - h0);
+            wt.slot_bst[s] = beg[u] + (uint32_t)(first - lo);
+            wt.slot_q[s] = q_anchor;
+            wt.slot_call[s] = c;
+            wt.hit_slot[s] = s + 1;
+          }
+          lo = hi;
+        }
+      }
+    }
+    __syncwarp();
+    {  // inclusive max-scan of the slot marks
+      constexpr int PER = TW / 32;
+      uint32_t *mark = wt.hit_slot;
+      const uint32_t base = lane * PER;
+      uint32_t run = 0;
+#pragma unroll
+      for (int i = 0; i < PER; i++)
+        if (base + i < nt) run = max(run, mark[base + i]);
+      uint32_t incl = run;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= (uint32_t)d) incl = max(incl, up);
+      }
+      uint32_t carry = __shfl_up_sync(0xffffffffu, incl, 1);
+      if (lane == 0) carry = 0;
+#pragma unroll
+      for (int i = 0; i < PER; i++)
+        if (base + i < nt) {
+          carry = max(carry, mark[base + i]);
+          mark[base + i] = carry;
+        }
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < nt; i += 32) {
+      uint32_t s = wt.hit_slot[i] - 1;
+      uint32_t r0 = __ldg(w.pos_table + wt.slot_bst[s] + (i - s)) + w.shape.size;
+      uint32_t q0 = wt.slot_q[s];
+      uint32_t hc = wt.slot_call[s];
+      const CallDev &cd = w.calls[hc];
+      uint32_t nr = min(w.rlen - r0, cd.qoff + cd.qlen - q0);
+      uint32_t nl = min(r0, q0 - cd.qoff);
+      wt.hit_r[i] = r0;
+      wt.hit_q[i] = q0;
+      wt.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
+      wt.hit_call[i] = hc;
+    }
+    __syncwarp();
+
+    // ---- the lockstep rounds ---------------------------------------------
+    // lane state: hit t of the tile, direction (0 right, 1 left), the next
+    // round's first base in the direction's packed halves, cells left to the
+    // edge or the cap, running sum and maximum, cells scored so far
+    bool have = false, capped = false;
+    uint32_t t = 0, dir = 0, rp = 0, qp = 0, n = 0, cells = 0, rcells = 0;
+    int32_t S = 0, M = 0, rmax = 0;
+    uint32_t cursor = 0;  // next unclaimed hit of the tile (the same in every lane)
+    // starts direction d of hit t
+    auto start = [&](uint32_t d) {
+      const uint32_t r0 = wt.hit_r[t], q0 = wt.hit_q[t], hn = wt.hit_n[t];
+      const uint32_t edge = d ? hn >> 16 : hn & 0xFFFFu;
+      capped = edge > a.cap;
+      n = capped ? a.cap : edge;
+      rp = d ? rlen - r0 : r0;
+      qp = d ? qtotal - q0 : q0;
+      dir = d;
+      S = 0;
+      M = 0;
+      cells = 0;
+    };
+    while (true) {
+      const unsigned need = __ballot_sync(0xffffffffu, !have);
+      if (need && cursor < nt) {
+        const uint32_t base = cursor;
+        cursor += (uint32_t)__popc(need);
+        if (!have) {
+          const uint32_t mine = base + (uint32_t)__popc(need & lanemask_lt());
+          if (mine < nt) {
+            have = true;
+            t = mine;
+            start(0);
+          }
+        }
+      }
+      if (!__any_sync(0xffffffffu, have)) break;
+      if (!have) n = 0;  // an idle lane scores an empty window at base 0
+      const uint32_t *rc = dir ? a2.ref2r : a2.ref2, *rm = dir ? a2.refmr : a2.refm;
+      const uint32_t *qc = dir ? a2.qry2r : a2.qry2, *qm = dir ? a2.qrymr : a2.qrym;
+      const uint32_t prp = have ? rp : 0u, pqp = have ? qp : 0u;
+      uint32_t Rl, Rh, RS, Ql, Qh, QS;
+      window32(rc, rm, prp, &Rl, &Rh, &RS);
+      window32(qc, qm, pqp, &Ql, &Qh, &QS);
+      // cells scored from the packed codes this round: up to the edge or cap,
+      // and before the first special base
+      const uint32_t v = min(n, (uint32_t)kRound);
+      const uint32_t sp = (RS | QS) & (v >= 32 ? 0xFFFFFFFFu : ((1u << v) - 1u));
+      const uint32_t vv = sp ? (uint32_t)(__ffs(sp) - 1) : v;
+
+      // every lane scores all 32 cells; per eight-cell group it keeps the
+      // state before the group and flags it when its final maximum minus its
+      // smallest sum exceeds xdrop (no flag: no cell of the group dropped)
+      int32_t Sg[4], Mg[4];
+      uint32_t flags = 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        uint32_t tw[4];
+        pair_words(h ? Rh : Rl, h ? Qh : Ql, tw);
+#pragma unroll
+        for (int gg = 0; gg < 2; gg++) {
+          const int g = 2 * h + gg;
+          Sg[g] = S;
+          Mg[g] = M;
+          int32_t lo = 0x7FFFFFFF;
+#pragma unroll
+          for (int i = 0; i < 8; i += 2) {
+            const int k = 8 * gg + i;
+            const int32_t S1 = wadd(S, cell_score(tbl, tw, k));
+            const int32_t S2 = wadd(S1, cell_score(tbl, tw, k + 1));
+            M = __vimax3_s32(M, S1, S2);
+            lo = __vimin3_s32(lo, S1, S2);
+            S = S2;
+          }
+          flags |= (uint32_t)((int32_t)((uint32_t)M - (uint32_t)lo) > X) << g;
+        }
+      }
+      // the groups to rescore exactly: flagged ones before the group holding
+      // the first unscored cell, and that group itself
+      const uint32_t gv = vv >> 3;
+      uint32_t todo = have ? (flags | (gv < 4 ? 1u << gv : 0u)) & ((2u << gv) - 1u) : 0u;
+      bool ended = false, dropped = false;
+      int32_t res = 0;
+      uint32_t used = kRound;
+      int32_t Sf = S, Mf = M;  // state after the round's scored cells
+      while (__any_sync(0xffffffffu, todo != 0)) {
+        if (todo) {
+          const uint32_t g = (uint32_t)(__ffs(todo) - 1);
+          todo &= todo - 1;
+          int32_t Se = Sg[0], Me = Mg[0];
+#pragma unroll
+          for (int x = 1; x < 4; x++)
+            if (g == (uint32_t)x) {
+              Se = Sg[x];
+              Me = Mg[x];
+            }
+          const uint32_t hw = g >= 2 ? Rh : Rl, qw = g >= 2 ? Qh : Ql;
+          const uint32_t sh = (g & 1u) << 4;
+          uint32_t tw[4];
+          pair_words((hw >> sh) & 0xFFFFu, (qw >> sh) & 0xFFFFu, tw);
+          const uint32_t lim = g == gv ? vv - 8 * g : 8u;
+          uint32_t d = 8;
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            const int32_t Sx = wadd(Se, cell_score(tbl, tw, i));
+            const int32_t Mx = max(Me, Sx);
+            if ((uint32_t)i < lim && d == 8) {
+              if ((int32_t)((uint32_t)Mx - (uint32_t)Sx) > X) {
+                d = (uint32_t)i;
+              } else {
+                Se = Sx;
+                Me = Mx;
+              }
+            }
+          }
+          if (d < 8) {  // the first cell past xdrop: the extension ends there
+            ended = dropped = true;
+            res = Me;
+            used = 8 * g + d + 1;
+            todo = 0;
+          } else if (g == gv) {  // no drop up to the first unscored cell
+            Sf = Se;
+            Mf = Me;
+            used = vv;
+            todo = 0;
+          }
+        }
+      }
+      if (have && !dropped) {
+        if (vv < (uint32_t)kRound && vv < v) {
+          // a special base at cell vv: its score from the 8-bit codes
+          const uint32_t pr = rp + vv, pq = qp + vv;
+          const uint32_t r8 = dir ? rlen - 1u - pr : pr, q8 = dir ? qtotal - 1u - pq : pq;
+          const int32_t sc = sm.sub[w.ref[r8] * kNuc + w.qbuf[q8]];
+          const int32_t Sx = wadd(Sf, sc);
+          const int32_t Mx = max(Mf, Sx);
+          used = vv + 1;
+          if ((int32_t)((uint32_t)Mx - (uint32_t)Sx) > X) {
+            ended = dropped = true;
+            res = Mf;
+          } else {
+            Sf = Sx;
+            Mf = Mx;
+          }
+        }
+        if (!dropped) {
+          S = Sf;
+          M = Mf;
+          if (used >= n) {  // reached the edge or the cap
+            ended = true;
+            res = M;
+          }
+        }
+      }
+      if (have) {
+        cells += used;
+        rp += used;
+        qp += used;
+        n -= min(used, n);
+      }
+      if (ended) {
+        const bool spill = !dropped && capped;
+        if (spill) {
+          uint32_t at = atomicAdd(&a.tot->cand, 1u);
+          if (at < a.cand_cap)
+            a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
+                              wt.hit_q[t], wt.hit_call[t] | kLongFlag};
+          have = false;  // the exact kernel redoes both directions
+        } else if (dir == 0) {
+          rmax = res;
+          rcells = cells;
+          start(1);
+        } else {
+          cells_acc += cells + rcells;
+          const int32_t tot = wadd(rmax, res);
+          if (a.total_exact ? tot >= a.hspthresh : sat_i32((double)__int2float_rn(tot)) >= a.hspthresh) {
+            uint32_t at = atomicAdd(&a.tot->cand, 1u);
+            if (at < a.cand_cap)
+              a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
+                                wt.hit_q[t], wt.hit_call[t]};
+          }
+          have = false;
+        }
+      }
+    }
+  }
+  for (int d = 16; d > 0; d >>= 1) cells_acc += __shfl_down_sync(0xffffffffu, cells_acc, d);
+  if (lane == 0 && cells_acc) atomicAdd(&a.tot->cells, cells_acc);
+}
+
+}  // namespace hz

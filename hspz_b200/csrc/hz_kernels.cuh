@@ -40,6 +40,40 @@ __global__ void encode_kernel(const uint8_t *__restrict__ ascii, uint64_t n, uin
 }
 
 // ---------------------------------------------------------------------------
+// 2-bit packing for the score gate.  A packed sequence is one logical run of
+// 2 * half bases: the block forward in [0, half) and read backwards in
+// [half, 2 * half) (base half + i is base n - 1 - i), so a left extension
+// walks the reversed half forwards with the same code as a right one.  ACGT
+// (codes 0..3) take 2 bits each, 16 bases per word, base i at bits
+// 2 (i % 16); every other code (soft-masked, N, other, separator) packs as 0
+// and sets its bit in the special mask (32 bases per word, base i at bit
+// i % 32).  Positions past the block in each half are 0 and not special;
+// extensions never score them.  One thread per 32 packed bases.
+__global__ void pack2_kernel(const uint8_t *__restrict__ codes, uint64_t n, uint64_t half,
+                             uint32_t *__restrict__ code2, uint32_t *__restrict__ special) {
+  const uint64_t blocks = (2 * half) / 32;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < blocks; b += stride) {
+    uint32_t lo = 0, hi = 0, sp = 0;
+    const uint64_t o0 = b * 32;
+    const bool rev = o0 >= half;
+#pragma unroll 4
+    for (uint32_t i = 0; i < 32; i++) {
+      const uint64_t o = (rev ? o0 - half : o0) + i;
+      if (o >= n) break;
+      const uint32_t c = codes[rev ? n - 1 - o : o];
+      const uint32_t bits = c < 4 ? c : 0u;
+      if (i < 16) lo |= bits << (2 * i);
+      else hi |= bits << (2 * (i - 16));
+      sp |= (uint32_t)(c >= 4) << i;
+    }
+    code2[2 * b] = lo;
+    code2[2 * b + 1] = hi;
+    special[b] = sp;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Spaced-seed hash on device codes: INVALID unless every base of the window
 // is uppercase ACGT (code < 4); else the care digits, first care position
 // most significant.  src/seed.rs:88-101.

@@ -423,6 +423,7 @@ __global__ void __launch_bounds__(kScopeThreads) scopes_kernel(WaveIn w, const u
 }  // namespace hz
 
 #include "hz_gate.cuh"
+#include "hz_gate2.cuh"
 
 namespace hz {
 

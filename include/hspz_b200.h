@@ -225,7 +225,10 @@ int hz_engine_profile_entry(hz_engine *e, uint32_t i, char *name, uint32_t name_
 int hz_engine_profile_reset(hz_engine *e);
 
 /* Launch-shape knobs (no reference counterpart; results never depend on
- * them): "gate_tile" (hits per gate warp tile: 64, 128, 256),
+ * them): "gate_version" (2, the default: the lockstep gate over 2-bit packed
+ * sequences, used whenever every ACGT score fits a signed byte; 1: the
+ * lane-refill gate over 8-bit codes, which also serves wider scores),
+ * "gate_tile" (hits per gate warp tile: 64, 128, 256),
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
  * "wave_positions" (seed positions per batched wave), "device_dedup" (1: the

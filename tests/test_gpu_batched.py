@@ -60,7 +60,8 @@ def test_batched_equals_plain_per_query(workload):
                                     dict(gate_tile=128, gate_blocks_per_sm=1), dict(gate_tile=256),
                                     dict(gate_tile=64), dict(device_dedup=0),
                                     dict(device_dedup=0, wave_positions=5_000), dict(graph=1),
-                                    dict(graph=1, wave_positions=20_000, gate_tile=64)])
+                                    dict(graph=1, wave_positions=20_000, gate_tile=64),
+                                    dict(gate_version=1), dict(gate_version=1, gate_tile=64, gate_cap=8)])
 def test_launch_shapes_do_not_change_results(workload, tuning):
     target, chunks = workload
     chunks = chunks[:16]

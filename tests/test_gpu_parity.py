@@ -93,13 +93,16 @@ def test_device_seed_table_is_byte_identical():
         assert np.array_equal(pos_d, pos_o), spec
 
 
-def test_config1_full_parity():
+@pytest.mark.parametrize("gate_version", [2, 1])
+def test_config1_full_parity(gate_version):
     """1 Mbp x 1 Mbp synthetic pair (41% GC, 10% soft-masked, 200 planted
-    segments at 15%), both strands: identical record list, order included."""
+    segments at 15%), both strands: identical record list, order included,
+    through the lockstep gate and through the lane-refill gate."""
     t, q = synth.config1(seed=1)
     sm = EngineConfig().sub_mat
     want, st_o = oracle_run(t, q, sm)
     with engine_for(sm) as e:
+        e.set_tuning(gate_version=gate_version)
         e.load_target(t)
         e.swap_query_ascii(q)
         got, st = e.run_pass()
