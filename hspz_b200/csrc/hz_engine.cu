@@ -751,6 +751,9 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
   w.per_pos = seeds ? 1u : e->per_pos(transitions);
   w.occ_cap = e->cfg.occ_cap;
   w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
+  const bool packed_q = e->qry_p.valid && e->shape.size <= 32 && e->qry_p.half >= e->qstore.len;
+  w.q2 = packed_q ? e->qry_p.code(0) : nullptr;
+  w.qm = packed_q ? e->qry_p.spec(0) : nullptr;
 
   for (int attempt = 0; attempt < 8; attempt++) {  // each rerun fixes every capacity it found short
     uint32_t scope_cap = std::max<uint32_t>(e->scope_cap, (uint32_t)n * 2 + 16);

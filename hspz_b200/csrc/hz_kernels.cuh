@@ -100,6 +100,27 @@ __device__ __forceinline__ uint32_t kmer_at(const uint8_t *__restrict__ codes, u
   return kmer;
 }
 
+// The same k-mer from a packed sequence (pack2_kernel's forward half), for
+// patterns of at most 32 bases: the window's special bits decide validity
+// with one masked test, and the care digits come out of one 64-bit window
+// of codes instead of one byte load each.
+__device__ __forceinline__ uint32_t kmer_packed(const uint32_t *__restrict__ code, const uint32_t *__restrict__ spec,
+                                                uint32_t x, const ShapeDev &sh) {
+  const uint32_t m = x >> 5;
+  const uint32_t sp = __funnelshift_r(__ldg(spec + m), __ldg(spec + m + 1), x & 31u);
+  if (sp & (sh.size >= 32 ? 0xFFFFFFFFu : ((1u << sh.size) - 1u))) return kInvalidKmer;
+  const uint32_t w = x >> 4, s = (x & 15u) << 1;
+  const uint32_t a0 = __ldg(code + w), a1 = __ldg(code + w + 1), a2 = __ldg(code + w + 2);
+  const uint32_t lo = __funnelshift_r(a0, a1, s), hi = __funnelshift_r(a1, a2, s);
+  uint32_t kmer = 0;
+  for (uint32_t t = 0; t < sh.kmer_size; t++) {
+    const uint32_t p = sh.pos[t];
+    const uint32_t d = p < 16 ? lo >> (2 * p) : hi >> (2 * p - 32);
+    kmer = (kmer << 2) | (d & 3u);
+  }
+  return kmer;
+}
+
 // ---------------------------------------------------------------------------
 // Seed table on device (SeedTable::build, src/seed.rs:135-180): k-mers of
 // the strided reference positions, compaction of the valid ones in position
