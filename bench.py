@@ -560,7 +560,34 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the oracle on a sample of the workload, checked against both forms
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and not args.no_cpu and args.cpu_query_bp and len(queries) == 1:
+        # a prefix of the one query as its own query block against bin 0: the
+        # oracle and both forms on exactly that block (for workloads whose
+        # first interval alone is too dense for a bounded CPU sample)
+        threads = os.cpu_count() or 1
+        sub = queries[0][: args.cpu_query_bp]
+        oc = CpuOracle(bins, [sub], occ_cap(args.config), threads)
+        picks = [(0, 0)]
+        o_recs, st, dt = oc.run(picks)
+        cpu = {"value": st["hits"] / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"bin 0 x the query's first {sub.size} bp as one query block ({st['calls']} "
+                         f"seed_and_filter calls, {st['hits']} hits, {dt:.1f} s)"}
+        with Engine(cfg, device=local_rank) as e0:
+            if tuning:
+                e0.set_tuning(**{k: tuning[k] for k in ("gate_tile", "gate_cap", "graph")})
+            e0.load_target(bins[0])
+            e0.stage_queries([sub])
+            gb, _ = e0.run_batched()
+            e0.select_query(0)
+            gp, _ = e0.run_pass()
+        checked = {"batched": same_records(gb, o_recs[0]), "plain": same_records(gp, o_recs[0])}
+        for f, ok in checked.items():
+            if not ok:
+                bad.append(f"{f} form != oracle on the query prefix")
+        parity["oracle"] = {"bin": 0, "query_prefix_bp": int(sub.size), "calls": int(st["calls"]),
+                            "hits": int(st["hits"]), "raw_hsps": int(st["raw_hsps"]), "hsps": int(st["hsps"]),
+                            "cells": int(st["cells"]), "sha256": parity_digest([o_recs[0]]), "equal": checked}
+    elif rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         oc = CpuOracle(bins, queries, occ_cap(args.config), threads)
         picks = sample_picks(args.config, queries, args.cpu_frac, seed=11)
@@ -844,6 +871,8 @@ def main():
                     help="share of the query bases the oracle checks (chunked workload)")
     ap.add_argument("--ref-frac", type=float, default=0.002,
                     help="reference arm: share of the query bases timed per step (chunked workload)")
+    ap.add_argument("--cpu-query-bp", type=int, default=0,
+                    help="one-query workloads: check the oracle on this prefix of the query as its own block")
     ap.add_argument("--plain-steps", type=int, default=3, help="timed steps of the plain form (at most --steps)")
     ap.add_argument("--e2e-steps", type=int, default=5, help="timed steps of the e2e leg (at most --steps)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving block of the default workload")
