@@ -324,7 +324,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
       uint32_t at = atomicAdd(&a.tot->cand, 1u);
       if (at < a.cand_cap)
         a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
-                          wt.hit_q[t], wt.hit_call[t] | kLongFlag};
+                          wt.hit_q[t], wt.hit_call[t] | kLongFlag, 0, 0};
       if (!LEFT) wt.hit_rmax[t] = kSpilled;  // the left pass skips it
     } else if (!LEFT) {
       wt.hit_rmax[t] = res;
@@ -336,7 +336,7 @@ __device__ __forceinline__ void gate_phase(const GateArgs &a, const char *subb, 
         uint32_t at = atomicAdd(&a.tot->cand, 1u);
         if (at < a.cand_cap)
           a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
-                            wt.hit_q[t], wt.hit_call[t]};
+                            wt.hit_q[t], wt.hit_call[t], wt.hit_rmax[t], res};
       }
     }
     have = false;

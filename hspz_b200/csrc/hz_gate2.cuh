@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
           uint32_t at = atomicAdd(&a.tot->cand, 1u);
           if (at < a.cand_cap)
             a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
-                              wt.hit_q[t], wt.hit_call[t] | kLongFlag};
+                              wt.hit_q[t], wt.hit_call[t] | kLongFlag, 0, 0};
           have = false;  // the exact kernel redoes both directions
         } else if (dir == 0) {
           rmax = res;
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
             uint32_t at = atomicAdd(&a.tot->cand, 1u);
             if (at < a.cand_cap)
               a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
-                                wt.hit_q[t], wt.hit_call[t]};
+                                wt.hit_q[t], wt.hit_call[t], rmax, res};
           }
           have = false;
         }

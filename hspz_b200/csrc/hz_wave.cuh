@@ -70,6 +70,8 @@ struct Cand {
   uint32_t r0;     // reference anchor
   uint32_t q0;     // query anchor, absolute in the query store
   uint32_t call;   // call index | kLongFlag
+  int32_t rmax;    // the gate's right and left maxima (not for a long candidate)
+  int32_t lmax;
 };
 constexpr uint32_t kLongFlag = 1u << 31;
 
@@ -431,10 +433,11 @@ __global__ void __launch_bounds__(kScopeThreads) scopes_kernel(WaveIn w, const u
 namespace hz {
 
 // ---------------------------------------------------------------------------
-// Exact extension, one warp per candidate: the reference's warp mapping of
-// find_hsps (src/gpu/kernels.rs:1279-1543) -- 32 cells per step, inclusive
-// sum and max scans, the first dropping lane by ballot, earliest-lane ties --
-// then the entropy correction and final threshold (:1555-1701).
+// Exact extension, one warp per candidate (find_hsps, src/gpu/kernels.rs:
+// 1279-1543): the positions of both maxima -- from the gate's maxima with one
+// sum scan per 32 cells, or, for a long candidate, the whole extension with
+// sum and maximum scans -- then the entropy correction and the final
+// threshold (:1555-1701).
 
 struct ExactArgs {
   const uint8_t *ref;
@@ -472,58 +475,11 @@ __device__ __forceinline__ int32_t warp_incl_max(int32_t v) {
   return v;
 }
 
-// One direction; returns (max, position) and adds the scored cells.
-template <bool LEFT>
-__device__ __forceinline__ void exact_dir(const uint8_t *ref, const uint8_t *qry, const int32_t *sub, int32_t X,
-                                          uint32_t r0, uint32_t q0, uint32_t nmax, uint32_t lane, int32_t *out_max,
-                                          int32_t *out_pos, unsigned long long *cells) {
-  int32_t prev_s = 0, prev_m = 0, prev_pos = LEFT ? 0 : -1;
-  for (uint32_t tile = 0;; tile += 32) {
-    uint32_t k = tile + lane;
-    int32_t sc = 0;
-    if (k < nmax) {
-      uint32_t rc = LEFT ? ref[r0 - 1 - k] : ref[r0 + k];
-      uint32_t qc = LEFT ? qry[q0 - 1 - k] : qry[q0 + k];
-      sc = sub[rc * kNuc + qc];
-    }
-    int32_t ts = (int32_t)((uint32_t)warp_incl_sum(sc, lane) + (uint32_t)prev_s);
-    int32_t cand = ts > prev_m ? ts : prev_m;
-    int32_t scanned = warp_incl_max(cand);
-    uint32_t dropped = __ballot_sync(0xffffffffu, (int32_t)((uint32_t)scanned - (uint32_t)ts) > X);
-    uint32_t first = dropped ? __ffs(dropped) - 1 : 32u;
-    int32_t mx = __shfl_sync(0xffffffffu, scanned, (first + 31) & 31);
-    if (first == 0) mx = prev_m;
-    int32_t pos;
-    if (mx == prev_m) {
-      pos = prev_pos;
-    } else {
-      uint32_t win = __ballot_sync(0xffffffffu, ts == mx && lane < first);
-      pos = (int32_t)(__ffs(win) - 1 + tile) + (LEFT ? 1 : 0);
-    }
-    if (dropped) {
-      *cells += min(tile + first + 1, nmax);
-      *out_max = mx;
-      *out_pos = pos;
-      return;
-    }
-    if (tile + 32 >= nmax) {  // the tile reached the edge
-      *cells += nmax;
-      *out_max = mx;
-      *out_pos = pos;
-      return;
-    }
-    prev_s = __shfl_sync(0xffffffffu, ts, 31);
-    prev_m = mx;
-    prev_pos = pos;
-  }
-}
-
-// The same direction with four consecutive cells per lane, 128 cells per
-// warp step: the lane sums its four cells, the warp scans the lane totals and
-// the lanes' largest sums, and the first dropping cell, the maximum before it
-// and that maximum's earliest position follow exactly as above.  Long
-// extensions (the occurrence-capped repeat tails and homologous runs that
-// reach the gate's cap) need a quarter of the scan steps.
+// One direction of a long candidate, four consecutive cells per lane, 128
+// cells per warp step: the lane sums its four cells, the warp scans the lane
+// totals and the lanes' largest sums; the first dropping cell (ballot), the
+// maximum before it and that maximum's earliest position (ballot of the lanes
+// holding it) follow; returns (max, position) and adds the scored cells.
 template <bool LEFT>
 __device__ __forceinline__ void exact_dir4(const uint8_t *ref, const uint8_t *qry, const int32_t *sub, int32_t X,
                                            uint32_t r0, uint32_t q0, uint32_t nmax, uint32_t lane, int32_t *out_max,
@@ -614,6 +570,33 @@ __device__ __forceinline__ void exact_dir4(const uint8_t *ref, const uint8_t *qr
   }
 }
 
+// The position of a direction's maximum when the maximum itself is already
+// known (the gate's, for a candidate whose extensions ended inside the gate):
+// the earliest cell whose running sum equals it -- the cell where the running
+// maximum first reached it, which lies before the dropping cell.  One sum scan
+// per 32 cells and a ballot; no maximum scan.  Right: the cell's offset (-1
+// when the maximum is 0); left: offset + 1 (0 when it is 0).
+template <bool LEFT>
+__device__ __forceinline__ int32_t exact_argmax(const uint8_t *ref, const uint8_t *qry, const int32_t *sub,
+                                                uint32_t r0, uint32_t q0, uint32_t nmax, int32_t mx, uint32_t lane) {
+  if (mx <= 0) return LEFT ? 0 : -1;
+  int32_t prev_s = 0;
+  for (uint32_t tile = 0; tile < nmax; tile += 32) {
+    const uint32_t k = tile + lane;
+    int32_t sc = 0;
+    if (k < nmax) {
+      const uint32_t rc = LEFT ? ref[r0 - 1 - k] : ref[r0 + k];
+      const uint32_t qc = LEFT ? qry[q0 - 1 - k] : qry[q0 + k];
+      sc = sub[rc * kNuc + qc];
+    }
+    const int32_t ts = (int32_t)((uint32_t)warp_incl_sum(sc, lane) + (uint32_t)prev_s);
+    const uint32_t at = __ballot_sync(0xffffffffu, k < nmax && ts == mx);
+    if (at) return (int32_t)(__ffs(at) - 1 + tile) + (LEFT ? 1 : 0);
+    prev_s = __shfl_sync(0xffffffffu, ts, 31);
+  }
+  return LEFT ? 0 : -1;  // not reached for a maximum of this extension
+}
+
 constexpr int kExactThreads = 128;
 
 __global__ void __launch_bounds__(kExactThreads) exact_kernel(ExactArgs a) {
@@ -636,10 +619,11 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(ExactArgs a) {
       exact_dir4<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos,
                         &cells);
       exact_dir4<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
-    } else {
-      exact_dir<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos,
-                       &cells);
-      exact_dir<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
+    } else {  // both maxima came from the gate; only their positions are left to find
+      rmax = cd.rmax;
+      lmax = cd.lmax;
+      rpos = exact_argmax<false>(a.ref, qry, sub, r0, q0, min(a.rlen - r0, call.qlen - q0), rmax, lane);
+      lpos = exact_argmax<true>(a.ref, qry, sub, r0, q0, min(r0, q0), lmax, lane);
     }
     if (is_long) cells_acc += cells;
     int32_t total = (int32_t)((uint32_t)rmax + (uint32_t)lmax);
