@@ -168,17 +168,47 @@ __global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, u
   __syncthreads();
   uint32_t c = s_c0;
   uint32_t valid = 0;
+  constexpr int kPer = kCountPerBlock / kCountThreads;
+  if (w.nbr_hits && w.per_pos > 1) {
+    // all of the thread's k-mers first, then their neighbourhood counts, so
+    // the count gathers of its positions are in flight together
+    uint32_t kmer[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; i++) {
+      const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
+      kmer[i] = kInvalidKmer;
+      if (p < w.npos) {
+        while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+        uint32_t qpos;
+        position_seed(w, w.calls[c], p, &qpos, &kmer[i]);
+      }
+    }
+    uint32_t sum[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; i++) {
+      sum[i] = 0;
+      if (kmer[i] != kInvalidKmer) {
+        valid++;
+        sum[i] = __ldg(w.nbr_hits + kmer[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; i++) {
+      const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
+      if (p < w.npos) pos_hits[p] = sum[i];
+    }
+    for (int d = 16; d > 0; d >>= 1) valid += __shfl_down_sync(0xffffffffu, valid, d);
+    if ((threadIdx.x & 31) == 0 && valid) atomicAdd(&tot->valid, (unsigned long long)valid);
+    return;
+  }
 #pragma unroll 1
-  for (int i = 0; i < kCountPerBlock / kCountThreads; i++) {
+  for (int i = 0; i < kPer; i++) {
     uint32_t p = p0 + i * kCountThreads + threadIdx.x;
     if (p >= w.npos) break;
     while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
     CallDev cd = w.calls[c];
     uint32_t qpos, kmer, sum = 0;
-    if (position_seed(w, cd, p, &qpos, &kmer) && w.nbr_hits && w.per_pos > 1) {
-      valid++;
-      sum = __ldg(w.nbr_hits + kmer);
-    } else if (kmer != kInvalidKmer) {
+    if (position_seed(w, cd, p, &qpos, &kmer)) {
       valid++;
       // every seed's bucket bounds are loaded before any is used, so the
       // loads are in flight together
