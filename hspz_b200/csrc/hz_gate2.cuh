@@ -15,7 +15,11 @@
 //     both directions are the same code;
 //   * after a round the lanes whose extension ended in it find the exact end
 //     cell and the maximum before it by rescoring one eight-cell group, and
-//     take the next hit-direction from the warp's tile.
+//     take the next hit-direction from the warp's tile;
+//   * a lane keeps its hit's anchors, call and left edge in registers, so
+//     when the tile runs out the warp sets up the next one at once while the
+//     lanes still on the old tile's hits carry on -- no lane waits for the
+//     slowest hit of a tile.
 // Bases that are not uppercase ACGT (soft-masked, N, other, separator) are
 // marked in a side mask; a round stops at the first one and that cell is
 // scored from the 8-bit codes and the full 8x8 table.
@@ -39,15 +43,14 @@ struct WarpTile2 {
   uint32_t slot_call[TW];
   uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
   uint32_t hit_r[TW];     // reference anchor
-  uint32_t hit_q[TW];     // query anchor (absolute)
   uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
-  uint32_t hit_call[TW];
+  int32_t grp[8][32];     // running sum and maximum of each lane at the start of each group of a round
 };
 
 template <int TW>
 struct Gate2Smem {
   int32_t sub[64];
-  int8_t tbl[4][256];  // score of the pair of codes a byte of a round's index word holds (see pair_byte)
+  int8_t tbl[4][256];  // score of the pair of codes a byte of a round's index word holds (see pair_words)
   WarpTile2<TW> warp[kGateWarps];
 };
 
@@ -118,18 +121,31 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
   const unsigned long long total = a.tot->hits;
   const uint32_t nz = a.tot->nz;
   const WaveIn &w = a.w;
-  while (true) {
+
+  // the tile the cursor hands hits out of (warp-uniform)
+  unsigned long long h0 = 0;
+  uint32_t nt = 0, cursor = 0;
+  bool tiles_done = false;
+  // Takes the next tile from the work queue and sets it up: the hits'
+  // anchors, edge distances and slots (query anchor, call).  Every lane takes
+  // part; lanes busy with an earlier tile's hits hold what they need of them
+  // in registers.
+  auto next_tile = [&]() {
     unsigned long long j = 0;
     if (lane == 0) j = atomicAdd(&a.tot->tiles, 1ull);
     j = __shfl_sync(0xffffffffu, j, 0);
-    const unsigned long long h0 = j * (unsigned long long)TW;
-    if (h0 >= total) break;
-    const uint32_t nt = (uint32_t)min((unsigned long long)TW, total - h0);
-    // ---- tile setup: the hits' anchors, edge distances and calls ----------
+    h0 = j * (unsigned long long)TW;
+    cursor = 0;
+    if (h0 >= total) {
+      tiles_done = true;
+      nt = 0;
+      return;
+    }
+    nt = (uint32_t)min((unsigned long long)TW, total - h0);
     const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
     const uint32_t e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
     uint32_t c = a.tile_call[j];
-    __syncwarp();  // the previous tile's lanes are done with its arrays
+    __syncwarp();  // every lane has read what it needs of the previous tile
     for (uint32_t i = lane; i < nt; i += 32) wt.hit_slot[i] = 0;
     __syncwarp();
     for (uint32_t k = k0 + lane; k <= e1; k += 32) {
@@ -192,199 +208,199 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
       uint32_t s = wt.hit_slot[i] - 1;
       uint32_t r0 = __ldg(w.pos_table + wt.slot_bst[s] + (i - s)) + w.shape.size;
       uint32_t q0 = wt.slot_q[s];
-      uint32_t hc = wt.slot_call[s];
-      const CallDev &cd = w.calls[hc];
+      const CallDev &cd = w.calls[wt.slot_call[s]];
       uint32_t nr = min(w.rlen - r0, cd.qoff + cd.qlen - q0);
       uint32_t nl = min(r0, q0 - cd.qoff);
       wt.hit_r[i] = r0;
-      wt.hit_q[i] = q0;
       wt.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
-      wt.hit_call[i] = hc;
     }
     __syncwarp();
+  };
 
-    // ---- the lockstep rounds ---------------------------------------------
-    // lane state: hit t of the tile, direction (0 right, 1 left), the next
-    // round's first base in the direction's packed halves, cells left to the
-    // edge or the cap, running sum and maximum, cells scored so far
-    bool have = false, capped = false;
-    uint32_t t = 0, dir = 0, rp = 0, qp = 0, n = 0, cells = 0, rcells = 0;
-    int32_t S = 0, M = 0, rmax = 0;
-    uint32_t cursor = 0;  // next unclaimed hit of the tile (the same in every lane)
-    // starts direction d of hit t
-    auto start = [&](uint32_t d) {
-      const uint32_t r0 = wt.hit_r[t], q0 = wt.hit_q[t], hn = wt.hit_n[t];
-      const uint32_t edge = d ? hn >> 16 : hn & 0xFFFFu;
-      capped = edge > a.cap;
-      n = capped ? a.cap : edge;
-      rp = d ? rlen - r0 : r0;
-      qp = d ? qtotal - q0 : q0;
-      dir = d;
-      S = 0;
-      M = 0;
-      cells = 0;
-    };
-    while (true) {
-      const unsigned need = __ballot_sync(0xffffffffu, !have);
-      if (need && cursor < nt) {
-        const uint32_t base = cursor;
-        cursor += (uint32_t)__popc(need);
-        if (!have) {
-          const uint32_t mine = base + (uint32_t)__popc(need & lanemask_lt());
-          if (mine < nt) {
-            have = true;
-            t = mine;
-            start(0);
-          }
+  // lane state: its hit (anchors, call, index in the wave, left edge), the
+  // direction (0 right, 1 left), the next round's first base in the
+  // direction's packed halves, cells left to the edge or the cap, running sum
+  // and maximum, cells scored so far in the direction
+  bool have = false, capped = false;
+  uint32_t dir = 0, rp = 0, qp = 0, n = 0, cells = 0, rcells = 0;
+  uint32_t hr0 = 0, hq0 = 0, hcall = 0, hnl = 0;
+  unsigned long long hidx = 0;
+  int32_t S = 0, M = 0, rmax = 0;
+  // starts direction d of the lane's hit over `edge` cells
+  auto start = [&](uint32_t d, uint32_t edge) {
+    capped = edge > a.cap;
+    n = capped ? a.cap : edge;
+    rp = d ? rlen - hr0 : hr0;
+    qp = d ? qtotal - hq0 : hq0;
+    dir = d;
+    S = 0;
+    M = 0;
+    cells = 0;
+  };
+  next_tile();
+  while (true) {
+    unsigned need = __ballot_sync(0xffffffffu, !have);
+    if (need && cursor >= nt && !tiles_done) next_tile();
+    if (need && cursor < nt) {
+      const uint32_t base = cursor;
+      cursor += (uint32_t)__popc(need);
+      if (!have) {
+        const uint32_t t = base + (uint32_t)__popc(need & lanemask_lt());
+        if (t < nt) {
+          have = true;
+          const uint32_t sl = wt.hit_slot[t] - 1, hn = wt.hit_n[t];
+          hr0 = wt.hit_r[t];
+          hq0 = wt.slot_q[sl];
+          hcall = wt.slot_call[sl];
+          hnl = hn >> 16;
+          hidx = h0 + t;
+          start(0, hn & 0xFFFFu);
         }
       }
-      if (!__any_sync(0xffffffffu, have)) break;
-      if (!have) n = 0;  // an idle lane scores an empty window at base 0
-      const uint32_t *rc = dir ? a2.ref2r : a2.ref2, *rm = dir ? a2.refmr : a2.refm;
-      const uint32_t *qc = dir ? a2.qry2r : a2.qry2, *qm = dir ? a2.qrymr : a2.qrym;
-      const uint32_t prp = have ? rp : 0u, pqp = have ? qp : 0u;
-      uint32_t Rl, Rh, RS, Ql, Qh, QS;
-      window32(rc, rm, prp, &Rl, &Rh, &RS);
-      window32(qc, qm, pqp, &Ql, &Qh, &QS);
-      // cells scored from the packed codes this round: up to the edge or cap,
-      // and before the first special base
-      const uint32_t v = min(n, (uint32_t)kRound);
-      const uint32_t sp = (RS | QS) & (v >= 32 ? 0xFFFFFFFFu : ((1u << v) - 1u));
-      const uint32_t vv = sp ? (uint32_t)(__ffs(sp) - 1) : v;
+    }
+    if (!__any_sync(0xffffffffu, have)) {
+      if (tiles_done) break;
+      continue;  // the next tile is set up at the top
+    }
+    if (!have) n = 0;  // an idle lane scores an empty window at base 0
+    const uint32_t *rc = dir ? a2.ref2r : a2.ref2, *rm = dir ? a2.refmr : a2.refm;
+    const uint32_t *qc = dir ? a2.qry2r : a2.qry2, *qm = dir ? a2.qrymr : a2.qrym;
+    const uint32_t prp = have ? rp : 0u, pqp = have ? qp : 0u;
+    uint32_t Rl, Rh, RS, Ql, Qh, QS;
+    window32(rc, rm, prp, &Rl, &Rh, &RS);
+    window32(qc, qm, pqp, &Ql, &Qh, &QS);
+    // cells scored from the packed codes this round: up to the edge or cap,
+    // and before the first special base
+    const uint32_t v = min(n, (uint32_t)kRound);
+    const uint32_t sp = (RS | QS) & (v >= 32 ? 0xFFFFFFFFu : ((1u << v) - 1u));
+    const uint32_t vv = sp ? (uint32_t)(__ffs(sp) - 1) : v;
 
-      // every lane scores all 32 cells; per eight-cell group it keeps the
-      // state before the group and flags it when its final maximum minus its
-      // smallest sum exceeds xdrop (no flag: no cell of the group dropped)
-      int32_t Sg[4], Mg[4];
-      uint32_t flags = 0;
+    // every lane scores all 32 cells; per eight-cell group it keeps the
+    // state before the group (in shared memory) and flags the group when its
+    // final maximum minus its smallest sum exceeds xdrop (no flag: no cell of
+    // the group dropped)
+    uint32_t flags = 0;
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+    for (int h = 0; h < 2; h++) {
+      uint32_t tw[4];
+      pair_words(h ? Rh : Rl, h ? Qh : Ql, tw);
+#pragma unroll
+      for (int gg = 0; gg < 2; gg++) {
+        const int g = 2 * h + gg;
+        wt.grp[2 * g][lane] = S;
+        wt.grp[2 * g + 1][lane] = M;
+        int32_t lo = 0x7FFFFFFF;
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+          const int k = 8 * gg + i;
+          const int32_t S1 = wadd(S, cell_score(tbl, tw, k));
+          const int32_t S2 = wadd(S1, cell_score(tbl, tw, k + 1));
+          M = __vimax3_s32(M, S1, S2);
+          lo = __vimin3_s32(lo, S1, S2);
+          S = S2;
+        }
+        flags |= (uint32_t)((int32_t)((uint32_t)M - (uint32_t)lo) > X) << g;
+      }
+    }
+    // the groups to rescore exactly: flagged ones before the group holding
+    // the first unscored cell, and that group itself
+    const uint32_t gv = vv >> 3;
+    uint32_t todo = have ? (flags | (gv < 4 ? 1u << gv : 0u)) & ((2u << gv) - 1u) : 0u;
+    bool ended = false, dropped = false;
+    int32_t res = 0;
+    uint32_t used = kRound;
+    int32_t Sf = S, Mf = M;  // state after the round's scored cells
+    while (__any_sync(0xffffffffu, todo != 0)) {
+      if (todo) {
+        const uint32_t g = (uint32_t)(__ffs(todo) - 1);
+        todo &= todo - 1;
+        int32_t Se = wt.grp[2 * g][lane], Me = wt.grp[2 * g + 1][lane];
+        const uint32_t hw = g >= 2 ? Rh : Rl, qw = g >= 2 ? Qh : Ql;
+        const uint32_t sh = (g & 1u) << 4;
         uint32_t tw[4];
-        pair_words(h ? Rh : Rl, h ? Qh : Ql, tw);
+        pair_words((hw >> sh) & 0xFFFFu, (qw >> sh) & 0xFFFFu, tw);
+        const uint32_t lim = g == gv ? vv - 8 * g : 8u;
+        uint32_t d = 8;
 #pragma unroll
-        for (int gg = 0; gg < 2; gg++) {
-          const int g = 2 * h + gg;
-          Sg[g] = S;
-          Mg[g] = M;
-          int32_t lo = 0x7FFFFFFF;
-#pragma unroll
-          for (int i = 0; i < 8; i += 2) {
-            const int k = 8 * gg + i;
-            const int32_t S1 = wadd(S, cell_score(tbl, tw, k));
-            const int32_t S2 = wadd(S1, cell_score(tbl, tw, k + 1));
-            M = __vimax3_s32(M, S1, S2);
-            lo = __vimin3_s32(lo, S1, S2);
-            S = S2;
-          }
-          flags |= (uint32_t)((int32_t)((uint32_t)M - (uint32_t)lo) > X) << g;
-        }
-      }
-      // the groups to rescore exactly: flagged ones before the group holding
-      // the first unscored cell, and that group itself
-      const uint32_t gv = vv >> 3;
-      uint32_t todo = have ? (flags | (gv < 4 ? 1u << gv : 0u)) & ((2u << gv) - 1u) : 0u;
-      bool ended = false, dropped = false;
-      int32_t res = 0;
-      uint32_t used = kRound;
-      int32_t Sf = S, Mf = M;  // state after the round's scored cells
-      while (__any_sync(0xffffffffu, todo != 0)) {
-        if (todo) {
-          const uint32_t g = (uint32_t)(__ffs(todo) - 1);
-          todo &= todo - 1;
-          int32_t Se = Sg[0], Me = Mg[0];
-#pragma unroll
-          for (int x = 1; x < 4; x++)
-            if (g == (uint32_t)x) {
-              Se = Sg[x];
-              Me = Mg[x];
-            }
-          const uint32_t hw = g >= 2 ? Rh : Rl, qw = g >= 2 ? Qh : Ql;
-          const uint32_t sh = (g & 1u) << 4;
-          uint32_t tw[4];
-          pair_words((hw >> sh) & 0xFFFFu, (qw >> sh) & 0xFFFFu, tw);
-          const uint32_t lim = g == gv ? vv - 8 * g : 8u;
-          uint32_t d = 8;
-#pragma unroll
-          for (int i = 0; i < 8; i++) {
-            const int32_t Sx = wadd(Se, cell_score(tbl, tw, i));
-            const int32_t Mx = max(Me, Sx);
-            if ((uint32_t)i < lim && d == 8) {
-              if ((int32_t)((uint32_t)Mx - (uint32_t)Sx) > X) {
-                d = (uint32_t)i;
-              } else {
-                Se = Sx;
-                Me = Mx;
-              }
+        for (int i = 0; i < 8; i++) {
+          const int32_t Sx = wadd(Se, cell_score(tbl, tw, i));
+          const int32_t Mx = max(Me, Sx);
+          if ((uint32_t)i < lim && d == 8) {
+            if ((int32_t)((uint32_t)Mx - (uint32_t)Sx) > X) {
+              d = (uint32_t)i;
+            } else {
+              Se = Sx;
+              Me = Mx;
             }
           }
-          if (d < 8) {  // the first cell past xdrop: the extension ends there
-            ended = dropped = true;
-            res = Me;
-            used = 8 * g + d + 1;
-            todo = 0;
-          } else if (g == gv) {  // no drop up to the first unscored cell
-            Sf = Se;
-            Mf = Me;
-            used = vv;
-            todo = 0;
-          }
+        }
+        if (d < 8) {  // the first cell past xdrop: the extension ends there
+          ended = dropped = true;
+          res = Me;
+          used = 8 * g + d + 1;
+          todo = 0;
+        } else if (g == gv) {  // no drop up to the first unscored cell
+          Sf = Se;
+          Mf = Me;
+          used = vv;
+          todo = 0;
         }
       }
-      if (have && !dropped) {
-        if (vv < (uint32_t)kRound && vv < v) {
-          // a special base at cell vv: its score from the 8-bit codes
-          const uint32_t pr = rp + vv, pq = qp + vv;
-          const uint32_t r8 = dir ? rlen - 1u - pr : pr, q8 = dir ? qtotal - 1u - pq : pq;
-          const int32_t sc = sm.sub[w.ref[r8] * kNuc + w.qbuf[q8]];
-          const int32_t Sx = wadd(Sf, sc);
-          const int32_t Mx = max(Mf, Sx);
-          used = vv + 1;
-          if ((int32_t)((uint32_t)Mx - (uint32_t)Sx) > X) {
-            ended = dropped = true;
-            res = Mf;
-          } else {
-            Sf = Sx;
-            Mf = Mx;
-          }
-        }
-        if (!dropped) {
-          S = Sf;
-          M = Mf;
-          if (used >= n) {  // reached the edge or the cap
-            ended = true;
-            res = M;
-          }
+    }
+    if (have && !dropped) {
+      if (vv < (uint32_t)kRound && vv < v) {
+        // a special base at cell vv: its score from the 8-bit codes
+        const uint32_t pr = rp + vv, pq = qp + vv;
+        const uint32_t r8 = dir ? rlen - 1u - pr : pr, q8 = dir ? qtotal - 1u - pq : pq;
+        const int32_t sc = sm.sub[w.ref[r8] * kNuc + w.qbuf[q8]];
+        const int32_t Sx = wadd(Sf, sc);
+        const int32_t Mx = max(Mf, Sx);
+        used = vv + 1;
+        if ((int32_t)((uint32_t)Mx - (uint32_t)Sx) > X) {
+          ended = dropped = true;
+          res = Mf;
+        } else {
+          Sf = Sx;
+          Mf = Mx;
         }
       }
-      if (have) {
-        cells += used;
-        rp += used;
-        qp += used;
-        n -= min(used, n);
+      if (!dropped) {
+        S = Sf;
+        M = Mf;
+        if (used >= n) {  // reached the edge or the cap
+          ended = true;
+          res = M;
+        }
       }
-      if (ended) {
-        const bool spill = !dropped && capped;
-        if (spill) {
+    }
+    if (have) {
+      cells += used;
+      rp += used;
+      qp += used;
+      n -= min(used, n);
+    }
+    if (ended) {
+      const bool spill = !dropped && capped;
+      if (spill) {
+        uint32_t at = atomicAdd(&a.tot->cand, 1u);
+        if (at < a.cand_cap)
+          a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), hidx), hr0, hq0,
+                            hcall | kLongFlag, 0, 0};
+        have = false;  // the exact kernel redoes both directions
+      } else if (dir == 0) {
+        rmax = res;
+        rcells = cells;
+        start(1, hnl);
+      } else {
+        cells_acc += cells + rcells;
+        const int32_t tot = wadd(rmax, res);
+        if (a.total_exact ? tot >= a.hspthresh : sat_i32((double)__int2float_rn(tot)) >= a.hspthresh) {
           uint32_t at = atomicAdd(&a.tot->cand, 1u);
           if (at < a.cand_cap)
-            a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
-                              wt.hit_q[t], wt.hit_call[t] | kLongFlag, 0, 0};
-          have = false;  // the exact kernel redoes both directions
-        } else if (dir == 0) {
-          rmax = res;
-          rcells = cells;
-          start(1);
-        } else {
-          cells_acc += cells + rcells;
-          const int32_t tot = wadd(rmax, res);
-          if (a.total_exact ? tot >= a.hspthresh : sat_i32((double)__int2float_rn(tot)) >= a.hspthresh) {
-            uint32_t at = atomicAdd(&a.tot->cand, 1u);
-            if (at < a.cand_cap)
-              a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), h0 + t), wt.hit_r[t],
-                                wt.hit_q[t], wt.hit_call[t], rmax, res};
-          }
-          have = false;
+            a.cand[at] = Cand{scope_of(a.scope_lo, min(a.tot->n_scopes, a.scope_cap), hidx), hr0, hq0, hcall,
+                              rmax, res};
         }
+        have = false;
       }
     }
   }
