@@ -126,14 +126,19 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
   unsigned long long h0 = 0;
   uint32_t nt = 0, cursor = 0;
   bool tiles_done = false;
+  // the next tile's index, claimed from the work queue once half of the
+  // current tile is handed out so that its latency is hidden (lane 0 holds it)
+  bool claimed = false;
+  unsigned long long claim = 0;
   // Takes the next tile from the work queue and sets it up: the hits'
   // anchors, edge distances and slots (query anchor, call).  Every lane takes
   // part; lanes busy with an earlier tile's hits hold what they need of them
   // in registers.
   auto next_tile = [&]() {
-    unsigned long long j = 0;
-    if (lane == 0) j = atomicAdd(&a.tot->tiles, 1ull);
+    unsigned long long j = claim;
+    if (!claimed && lane == 0) j = atomicAdd(&a.tot->tiles, 1ull);
     j = __shfl_sync(0xffffffffu, j, 0);
+    claimed = false;
     h0 = j * (unsigned long long)TW;
     cursor = 0;
     if (h0 >= total) {
@@ -239,6 +244,10 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
   };
   next_tile();
   while (true) {
+    if (!claimed && !tiles_done && 2 * cursor >= nt) {
+      if (lane == 0) claim = atomicAdd(&a.tot->tiles, 1ull);
+      claimed = true;
+    }
     unsigned need = __ballot_sync(0xffffffffu, !have);
     if (need && cursor >= nt && !tiles_done) next_tile();
     if (need && cursor < nt) {
@@ -319,6 +328,26 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
         const uint32_t sh = (g & 1u) << 4;
         uint32_t tw[4];
         pair_words((hw >> sh) & 0xFFFFu, (qw >> sh) & 0xFFFFu, tw);
+        if (a.late_max_safe && g != gv) {
+          // A full group.  No cell within seven after a dropping cell can
+          // raise the maximum (7 x the largest score <= xdrop), so the
+          // maximum before the drop is the group's final one; only the
+          // dropping cell is searched, by the drawdown D = M - S.
+          int32_t D = (int32_t)((uint32_t)Me - (uint32_t)Se);
+          uint32_t dm = 0;
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            D = max((int32_t)((uint32_t)D - (uint32_t)cell_score(tbl, tw, i)), 0);
+            dm |= (uint32_t)(D > X) << i;
+          }
+          if (dm) {
+            ended = dropped = true;
+            res = g < 3 ? wt.grp[2 * g + 3][lane] : M;
+            used = 8 * g + (uint32_t)(__ffs(dm) - 1) + 1;
+            todo = 0;
+          }  // else the flag was loose: the next flagged group is looked at
+          continue;
+        }
         const uint32_t lim = g == gv ? vv - 8 * g : 8u;
         uint32_t d = 8;
 #pragma unroll
