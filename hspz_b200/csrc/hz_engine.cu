@@ -486,20 +486,20 @@ bool gate2_usable(const hz_engine *e) {
 
 template <int TW> size_t gate2_smem() { return sizeof(Gate2Smem<TW>); }
 
-template <int TW, int MINB> int launch_gate2(hz_engine *e, const GateArgs &ga) {
+template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
   static bool configured[64] = {false};
   static std::mutex mu;  // serving workers launch from several host threads
   size_t smem = gate2_smem<TW>();
   {
     std::lock_guard<std::mutex> lock(mu);
     if (!configured[e->device & 63]) {
-      CK(cudaFuncSetAttribute(gate2_kernel<TW, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CK(cudaFuncSetAttribute(gate2_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       configured[e->device & 63] = true;
     }
   }
   int per_sm = e->gate_blocks_per_sm;
-  if (per_sm <= 0 || per_sm > MINB) {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate2_kernel<TW, MINB>, kGateThreads, smem));
+  if (per_sm <= 0) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate2_kernel<TW>, kGateThreads, smem));
     if (per_sm < 1) per_sm = 1;
   }
   Gate2Args a2;
@@ -514,7 +514,7 @@ template <int TW, int MINB> int launch_gate2(hz_engine *e, const GateArgs &ga) {
   a2.qrymr = e->qry_p.spec(1);
   a2.qtotal = (uint32_t)e->qstore.len;
   unsigned grid = (unsigned)(e->sm_count * per_sm);
-  return e->launch("gate", [&] { gate2_kernel<TW, MINB><<<grid, kGateThreads, smem, e->st>>>(a2); });
+  return e->launch("gate", [&] { gate2_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(a2); });
 }
 
 template <int TW> int launch_gate(hz_engine *e, const GateArgs &ga) {
@@ -816,10 +816,9 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       ga.tile_call = e->tile_call.p;
       if (gate2_usable(e)) {
         switch (e->gate_tile) {
-          // five blocks per SM asked for: the variant held to 48 registers
-          case 64: TRY((e->gate_blocks_per_sm >= 5 ? launch_gate2<64, 5>(e, ga) : launch_gate2<64, 4>(e, ga))); break;
-          case 256: TRY((launch_gate2<256, 4>(e, ga))); break;
-          default: TRY((e->gate_blocks_per_sm >= 5 ? launch_gate2<128, 5>(e, ga) : launch_gate2<128, 4>(e, ga))); break;
+          case 64: TRY(launch_gate2<64>(e, ga)); break;
+          case 256: TRY(launch_gate2<256>(e, ga)); break;
+          default: TRY(launch_gate2<128>(e, ga)); break;
         }
       } else {
         switch (e->gate_tile) {

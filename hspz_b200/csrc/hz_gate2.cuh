@@ -98,10 +98,8 @@ __device__ __forceinline__ void window32(const uint32_t *code, const uint32_t *s
   *sp = __funnelshift_r(__ldg(spec + m), __ldg(spec + m + 1), p & 31u);
 }
 
-// MINB: blocks per SM the registers are held to (4: 64 registers, 5: 48 with
-// a few spilled)
-template <int TW, int MINB>
-__global__ void __launch_bounds__(kGateThreads, MINB) gate2_kernel(Gate2Args a2) {
+template <int TW>
+__global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
   static_assert(TW % 32 == 0, "a warp tile is a multiple of 32 hits");
   const GateArgs &a = a2.g;
   extern __shared__ __align__(16) unsigned char smem_raw[];
