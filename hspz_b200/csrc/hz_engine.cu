@@ -231,14 +231,12 @@ unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 148u * 64u) {
 // the forward half and the reversed half, each `half` bases, codes and
 // special masks.
 struct Packed {
-  DBuf<uint32_t> code2, special;
+  DBuf<uint4> blk;  // one 16-byte record per 32 bases
   uint64_t half = 0;
   bool valid = false;
-  const uint32_t *code(int rev) const { return code2.p + (rev ? half / 16 : 0); }
-  const uint32_t *spec(int rev) const { return special.p + (rev ? half / 32 : 0); }
+  const uint4 *half_ptr(int rev) const { return blk.p + (rev ? half / 32 : 0); }
   void release() {
-    code2.release();
-    special.release();
+    blk.release();
     valid = false;
   }
 };
@@ -460,13 +458,11 @@ int pack_seq(hz_engine *e, const uint8_t *codes, uint64_t n, Packed *p) {
   p->valid = false;
   p->half = (n + 64 + 31) & ~31ull;
   const uint64_t blocks = 2 * p->half / 32;
-  TRY(p->code2.ensure(2 * blocks + 8, s));
-  TRY(p->special.ensure(blocks + 8, s));
-  CK(cudaMemsetAsync(p->code2.p + 2 * blocks, 0, 8 * sizeof(uint32_t), s));
-  CK(cudaMemsetAsync(p->special.p + blocks, 0, 8 * sizeof(uint32_t), s));
-  uint32_t *c2 = p->code2.p, *sp = p->special.p;
+  TRY(p->blk.ensure(blocks + 4, s));
+  CK(cudaMemsetAsync(p->blk.p + blocks, 0, 4 * sizeof(uint4), s));  // read by windows past the end
+  uint4 *bk = p->blk.p;
   const uint64_t half = p->half;
-  TRY(e->launch("pack", [&] { pack2_kernel<<<grid_for(blocks, 256), 256, 0, s>>>(codes, n, half, c2, sp); }));
+  TRY(e->launch("pack", [&] { pack2_kernel<<<grid_for(blocks, 256), 256, 0, s>>>(codes, n, half, bk); }));
   p->valid = true;
   return HZ_OK;
 }
@@ -504,14 +500,10 @@ template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
   }
   Gate2Args a2;
   a2.g = ga;
-  a2.ref2 = e->ref_p.code(0);
-  a2.refm = e->ref_p.spec(0);
-  a2.ref2r = e->ref_p.code(1);
-  a2.refmr = e->ref_p.spec(1);
-  a2.qry2 = e->qry_p.code(0);
-  a2.qrym = e->qry_p.spec(0);
-  a2.qry2r = e->qry_p.code(1);
-  a2.qrymr = e->qry_p.spec(1);
+  a2.ref = e->ref_p.half_ptr(0);
+  a2.refr = e->ref_p.half_ptr(1);
+  a2.qry = e->qry_p.half_ptr(0);
+  a2.qryr = e->qry_p.half_ptr(1);
   a2.qtotal = (uint32_t)e->qstore.len;
   unsigned grid = (unsigned)(e->sm_count * per_sm);
   return e->launch("gate", [&] { gate2_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(a2); });
@@ -752,8 +744,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
   w.occ_cap = e->cfg.occ_cap;
   w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
   const bool packed_q = e->qry_p.valid && e->shape.size <= 32 && e->qry_p.half >= e->qstore.len;
-  w.q2 = packed_q ? e->qry_p.code(0) : nullptr;
-  w.qm = packed_q ? e->qry_p.spec(0) : nullptr;
+  w.qp2 = packed_q ? e->qry_p.half_ptr(0) : nullptr;
 
   for (int attempt = 0; attempt < 8; attempt++) {  // each rerun fixes every capacity it found short
     uint32_t scope_cap = std::max<uint32_t>(e->scope_cap, (uint32_t)n * 2 + 16);
@@ -2214,7 +2205,7 @@ template <typename T> uint64_t dbytes(const DBuf<T> &b) { return b.p ? b.cap * s
 // Device bytes an engine's own working buffers hold: its query store (unless
 // it borrows another engine's) and every wave and dedup buffer.
 uint64_t wave_footprint(const hz_engine *w) {
-  uint64_t b = w->aliases_query ? 0 : dbytes(w->qstore.buf) + dbytes(w->qry_p.code2) + dbytes(w->qry_p.special);
+  uint64_t b = w->aliases_query ? 0 : dbytes(w->qstore.buf) + dbytes(w->qry_p.blk);
   b += dbytes(w->qascii) + dbytes(w->calls) + dbytes(w->pos_hits) + dbytes(w->np_pos) + dbytes(w->call_nz_lo) +
        dbytes(w->scope_call) + dbytes(w->raw_scope) + dbytes(w->tile_first) + dbytes(w->tile_call) +
        dbytes(w->np_excl) + dbytes(w->call_hit_lo) + dbytes(w->scope_lo) + dbytes(w->np_partial) +

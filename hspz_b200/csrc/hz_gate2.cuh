@@ -8,7 +8,7 @@
 //     cells, every lane the same 32 cells' worth of instructions whether its
 //     extension ends in the round or not;
 //   * the reference and query are read 2 bits per base (pack2_kernel), so a
-//     round's cells are two 64-bit windows (five word loads per sequence) and
+//     round's cells are two 64-bit windows (two 16-byte loads per sequence) and
 //     a cell's substitution score is one byte extract and one shared-memory
 //     byte load from a table indexed by the pair of codes;
 //   * a left extension walks the reversed copy of each sequence forwards, so
@@ -56,10 +56,9 @@ struct Gate2Smem {
 
 struct Gate2Args {
   GateArgs g;
-  // packed sequences: codes and special masks of the forward half and of the
-  // reversed half (pack2_kernel)
-  const uint32_t *ref2, *refm, *ref2r, *refmr;
-  const uint32_t *qry2, *qrym, *qry2r, *qrymr;
+  // packed sequences (pack2_kernel's records): the forward and the reversed
+  // half of the reference and of the query store
+  const uint4 *ref, *refr, *qry, *qryr;
   uint32_t qtotal;  // bases of the query store (the reversed query half is it read backwards)
 };
 
@@ -86,17 +85,6 @@ __device__ __forceinline__ int32_t cell_score(const int8_t (*tbl)[256], const ui
 }
 
 __device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
-
-// 32 bases of a packed half starting at base p: codes (two words) and specials.
-__device__ __forceinline__ void window32(const uint32_t *code, const uint32_t *spec, uint32_t p, uint32_t *lo,
-                                         uint32_t *hi, uint32_t *sp) {
-  const uint32_t w = p >> 4, sh = (p & 15u) << 1;
-  const uint32_t a0 = __ldg(code + w), a1 = __ldg(code + w + 1), a2 = __ldg(code + w + 2);
-  *lo = __funnelshift_r(a0, a1, sh);
-  *hi = __funnelshift_r(a1, a2, sh);
-  const uint32_t m = p >> 5;
-  *sp = __funnelshift_r(__ldg(spec + m), __ldg(spec + m + 1), p & 31u);
-}
 
 template <int TW>
 __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
@@ -272,12 +260,10 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
       continue;  // the next tile is set up at the top
     }
     if (!have) n = 0;  // an idle lane scores an empty window at base 0
-    const uint32_t *rc = dir ? a2.ref2r : a2.ref2, *rm = dir ? a2.refmr : a2.refm;
-    const uint32_t *qc = dir ? a2.qry2r : a2.qry2, *qm = dir ? a2.qrymr : a2.qrym;
     const uint32_t prp = have ? rp : 0u, pqp = have ? qp : 0u;
     uint32_t Rl, Rh, RS, Ql, Qh, QS;
-    window32(rc, rm, prp, &Rl, &Rh, &RS);
-    window32(qc, qm, pqp, &Ql, &Qh, &QS);
+    window32(dir ? a2.refr : a2.ref, prp, &Rl, &Rh, &RS);
+    window32(dir ? a2.qryr : a2.qry, pqp, &Ql, &Qh, &QS);
     // cells scored from the packed codes this round: up to the edge or cap,
     // and before the first special base
     const uint32_t v = min(n, (uint32_t)kRound);

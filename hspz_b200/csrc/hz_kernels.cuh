@@ -40,17 +40,18 @@ __global__ void encode_kernel(const uint8_t *__restrict__ ascii, uint64_t n, uin
 }
 
 // ---------------------------------------------------------------------------
-// 2-bit packing for the score gate.  A packed sequence is one logical run of
-// 2 * half bases: the block forward in [0, half) and read backwards in
-// [half, 2 * half) (base half + i is base n - 1 - i), so a left extension
-// walks the reversed half forwards with the same code as a right one.  ACGT
-// (codes 0..3) take 2 bits each, 16 bases per word, base i at bits
-// 2 (i % 16); every other code (soft-masked, N, other, separator) packs as 0
-// and sets its bit in the special mask (32 bases per word, base i at bit
-// i % 32).  Positions past the block in each half are 0 and not special;
-// extensions never score them.  One thread per 32 packed bases.
+// 2-bit packing for the score gate and the seed windows.  A packed sequence is
+// one logical run of 2 * half bases: the block forward in [0, half) and read
+// backwards in [half, 2 * half) (base half + i is base n - 1 - i), so a left
+// extension walks the reversed half forwards with the same code as a right
+// one.  Every 32 bases are one 16-byte record: x, y = the ACGT codes (2 bits
+// per base, base i at bits 2 (i % 16) of x for i < 16, of y above), z = the
+// special mask (bit i set when base i is not uppercase ACGT -- soft-masked,
+// N, other or separator -- whose code packs as 0), w = 0.  Positions past the
+// block in each half are 0 and not special; extensions never score them.  One
+// record per thread.
 __global__ void pack2_kernel(const uint8_t *__restrict__ codes, uint64_t n, uint64_t half,
-                             uint32_t *__restrict__ code2, uint32_t *__restrict__ special) {
+                             uint4 *__restrict__ blk) {
   const uint64_t blocks = (2 * half) / 32;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < blocks; b += stride) {
@@ -67,10 +68,22 @@ __global__ void pack2_kernel(const uint8_t *__restrict__ codes, uint64_t n, uint
       else hi |= bits << (2 * (i - 16));
       sp |= (uint32_t)(c >= 4) << i;
     }
-    code2[2 * b] = lo;
-    code2[2 * b + 1] = hi;
-    special[b] = sp;
+    blk[b] = make_uint4(lo, hi, sp, 0u);
   }
+}
+
+// The 32 bases of a packed half that start at base p: their codes (lo: the
+// first 16, hi: the next 16) and their special bits, from the two 16-byte
+// records that hold them.
+__device__ __forceinline__ void window32(const uint4 *__restrict__ blk, uint32_t p, uint32_t *lo, uint32_t *hi,
+                                         uint32_t *sp) {
+  const uint4 A = __ldg(blk + (p >> 5)), B = __ldg(blk + (p >> 5) + 1);
+  const uint32_t o = p & 31u, sh = (o & 15u) << 1;
+  const bool upper = o >= 16;  // the window starts in the record's second code word
+  const uint32_t w0 = upper ? A.y : A.x, w1 = upper ? B.x : A.y, w2 = upper ? B.y : B.x;
+  *lo = __funnelshift_r(w0, w1, sh);
+  *hi = __funnelshift_r(w1, w2, sh);
+  *sp = __funnelshift_r(A.z, B.z, o);
 }
 
 // ---------------------------------------------------------------------------
@@ -104,14 +117,10 @@ __device__ __forceinline__ uint32_t kmer_at(const uint8_t *__restrict__ codes, u
 // patterns of at most 32 bases: the window's special bits decide validity
 // with one masked test, and the care digits come out of one 64-bit window
 // of codes instead of one byte load each.
-__device__ __forceinline__ uint32_t kmer_packed(const uint32_t *__restrict__ code, const uint32_t *__restrict__ spec,
-                                                uint32_t x, const ShapeDev &sh) {
-  const uint32_t m = x >> 5;
-  const uint32_t sp = __funnelshift_r(__ldg(spec + m), __ldg(spec + m + 1), x & 31u);
+__device__ __forceinline__ uint32_t kmer_packed(const uint4 *__restrict__ blk, uint32_t x, const ShapeDev &sh) {
+  uint32_t lo, hi, sp;
+  window32(blk, x, &lo, &hi, &sp);
   if (sp & (sh.size >= 32 ? 0xFFFFFFFFu : ((1u << sh.size) - 1u))) return kInvalidKmer;
-  const uint32_t w = x >> 4, s = (x & 15u) << 1;
-  const uint32_t a0 = __ldg(code + w), a1 = __ldg(code + w + 1), a2 = __ldg(code + w + 2);
-  const uint32_t lo = __funnelshift_r(a0, a1, s), hi = __funnelshift_r(a1, a2, s);
   uint32_t kmer = 0;
   for (uint32_t t = 0; t < sh.kmer_size; t++) {
     const uint32_t p = sh.pos[t];

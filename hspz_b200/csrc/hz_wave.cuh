@@ -45,8 +45,8 @@ struct WaveIn {
   uint32_t occ_cap;
   const uint32_t *nbr_hits;  // per k-mer hits of all 1 + kmer_size seeds, or null
   // the query store packed 2 bits per base (forward half of pack2_kernel's
-  // layout): codes and special masks, or null to read the 8-bit codes
-  const uint32_t *q2, *qm;
+  // records), or null to read the 8-bit codes
+  const uint4 *qp2;
 };
 
 // Device-side counters of a wave.
@@ -95,7 +95,7 @@ __device__ __forceinline__ bool position_seed(const WaveIn &w, const CallDev &c,
     return true;
   }
   *qpos = c.start + (p - c.pos_off);
-  *kmer = w.q2 ? kmer_packed(w.q2, w.qm, c.qoff + *qpos, w.shape) : kmer_at(w.qbuf + c.qoff, *qpos, w.shape);
+  *kmer = w.qp2 ? kmer_packed(w.qp2, c.qoff + *qpos, w.shape) : kmer_at(w.qbuf + c.qoff, *qpos, w.shape);
   return *kmer != kInvalidKmer;
 }
 
