@@ -34,7 +34,35 @@
 
 namespace hz {
 
-constexpr int kRound = 32;  // cells a lane scores per round
+constexpr int kRound = 48;             // cells a lane scores per round
+constexpr int kChunks = kRound / 16;   // 16-cell code words per sequence in a round
+constexpr int kGroups = kRound / 8;    // eight-cell groups per round
+
+// The kRound bases of a packed half that start at base p: their codes, 16
+// per word, and their special bits (cells 0..31 in *sp_lo, the rest in
+// *sp_hi), from the 16-byte records that hold them.
+__device__ __forceinline__ void window_round(const uint4 *__restrict__ blk, uint32_t p, uint32_t code[kChunks],
+                                             uint32_t *sp_lo, uint32_t *sp_hi) {
+  constexpr int kRec = (kRound + 31) / 32 + 1;
+  uint4 r[kRec];
+#pragma unroll
+  for (int i = 0; i < kRec; i++) r[i] = __ldg(blk + (p >> 5) + i);
+  uint32_t c[2 * kRec];
+#pragma unroll
+  for (int i = 0; i < kRec; i++) {
+    c[2 * i] = r[i].x;
+    c[2 * i + 1] = r[i].y;
+  }
+  const uint32_t o = p & 31u, sh = (o & 15u) << 1;
+  const bool upper = o >= 16;  // the window starts in a record's second code word
+  uint32_t cs[kChunks + 1];
+#pragma unroll
+  for (int k = 0; k <= kChunks; k++) cs[k] = upper ? c[k + 1] : c[k];
+#pragma unroll
+  for (int k = 0; k < kChunks; k++) code[k] = __funnelshift_r(cs[k], cs[k + 1], sh);
+  *sp_lo = __funnelshift_r(r[0].z, r[1].z, o);
+  *sp_hi = kRound > 32 ? __funnelshift_r(r[1].z, r[kRec - 1].z, o) : 0u;
+}
 
 template <int TW>
 struct WarpTile2 {
@@ -44,7 +72,7 @@ struct WarpTile2 {
   uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
   uint32_t hit_r[TW];     // reference anchor
   uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
-  int32_t grp[8][32];     // running sum and maximum of each lane at the start of each group of a round
+  int32_t grp[2 * kGroups][32];  // running sum and maximum of each lane at the start of each group of a round
 };
 
 template <int TW>
@@ -261,24 +289,25 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
     }
     if (!have) n = 0;  // an idle lane scores an empty window at base 0
     const uint32_t prp = have ? rp : 0u, pqp = have ? qp : 0u;
-    uint32_t Rl, Rh, RS, Ql, Qh, QS;
-    window32(dir ? a2.refr : a2.ref, prp, &Rl, &Rh, &RS);
-    window32(dir ? a2.qryr : a2.qry, pqp, &Ql, &Qh, &QS);
+    uint32_t Rc[kChunks], Qc[kChunks], RS0, RS1, QS0, QS1;
+    window_round(dir ? a2.refr : a2.ref, prp, Rc, &RS0, &RS1);
+    window_round(dir ? a2.qryr : a2.qry, pqp, Qc, &QS0, &QS1);
     // cells scored from the packed codes this round: up to the edge or cap,
     // and before the first special base
     const uint32_t v = min(n, (uint32_t)kRound);
-    const uint32_t sp = (RS | QS) & (v >= 32 ? 0xFFFFFFFFu : ((1u << v) - 1u));
-    const uint32_t vv = sp ? (uint32_t)(__ffs(sp) - 1) : v;
+    const uint32_t sp0 = (RS0 | QS0) & (v >= 32 ? 0xFFFFFFFFu : ((1u << v) - 1u));
+    const uint32_t sp1 = (RS1 | QS1) & (v > 32 ? ((1u << (v - 32)) - 1u) : 0u);
+    const uint32_t vv = sp0 ? (uint32_t)(__ffs(sp0) - 1) : sp1 ? 32u + (uint32_t)(__ffs(sp1) - 1) : v;
 
-    // every lane scores all 32 cells; per eight-cell group it keeps the
+    // every lane scores all kRound cells; per eight-cell group it keeps the
     // state before the group (in shared memory) and flags the group when its
     // final maximum minus its smallest sum exceeds xdrop (no flag: no cell of
     // the group dropped)
     uint32_t flags = 0;
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
+    for (int h = 0; h < kChunks; h++) {
       uint32_t tw[4];
-      pair_words(h ? Rh : Rl, h ? Qh : Ql, tw);
+      pair_words(Rc[h], Qc[h], tw);
 #pragma unroll
       for (int gg = 0; gg < 2; gg++) {
         const int g = 2 * h + gg;
@@ -300,7 +329,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
     // the groups to rescore exactly: flagged ones before the group holding
     // the first unscored cell, and that group itself
     const uint32_t gv = vv >> 3;
-    uint32_t todo = have ? (flags | (gv < 4 ? 1u << gv : 0u)) & ((2u << gv) - 1u) : 0u;
+    uint32_t todo = have ? (flags | (gv < (uint32_t)kGroups ? 1u << gv : 0u)) & ((2u << gv) - 1u) : 0u;
     bool ended = false, dropped = false;
     int32_t res = 0;
     uint32_t used = kRound;
@@ -310,7 +339,9 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
         const uint32_t g = (uint32_t)(__ffs(todo) - 1);
         todo &= todo - 1;
         int32_t Se = wt.grp[2 * g][lane], Me = wt.grp[2 * g + 1][lane];
-        const uint32_t hw = g >= 2 ? Rh : Rl, qw = g >= 2 ? Qh : Ql;
+        const uint32_t ch = g >> 1;  // the code word holding the group (constant indices keep Rc, Qc in registers)
+        const uint32_t hw = ch == 0 ? Rc[0] : ch == 1 ? Rc[1] : Rc[kChunks - 1];
+        const uint32_t qw = ch == 0 ? Qc[0] : ch == 1 ? Qc[1] : Qc[kChunks - 1];
         const uint32_t sh = (g & 1u) << 4;
         uint32_t tw[4];
         pair_words((hw >> sh) & 0xFFFFu, (qw >> sh) & 0xFFFFu, tw);
@@ -328,7 +359,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
           }
           if (dm) {
             ended = dropped = true;
-            res = g < 3 ? wt.grp[2 * g + 3][lane] : M;
+            res = g + 1 < (uint32_t)kGroups ? wt.grp[2 * g + 3][lane] : M;
             used = 8 * g + (uint32_t)(__ffs(dm) - 1) + 1;
             todo = 0;
           }  // else the flag was loose: the next flagged group is looked at
