@@ -4,11 +4,14 @@
 // bound of every hit, src/gpu/kernels.rs:521-1057 -- organised so that a
 // warp's 32 lanes run one instruction stream without divergence in the hot
 // loop:
-//   * a lane owns one hit-direction at a time and scores it in rounds of 32
-//     cells, every lane the same 32 cells' worth of instructions whether its
-//     extension ends in the round or not;
+//   * a lane owns one hit-direction at a time and scores it in rounds of 48
+//     cells (kRound), every lane the same 48 cells' worth of instructions
+//     whether its extension ends in the round or not (random hits end after
+//     ~23 cells to the right and ~41 to the left, so most directions take one
+//     round);
 //   * the reference and query are read 2 bits per base (pack2_kernel), so a
-//     round's cells are two 64-bit windows (two 16-byte loads per sequence) and
+//     round's cells are three 16-cell code words per sequence (three 16-byte
+//     loads) and
 //     a cell's substitution score is one byte extract and one shared-memory
 //     byte load from a table indexed by the pair of codes;
 //   * a left extension walks the reversed copy of each sequence forwards, so
