@@ -761,8 +761,10 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       CK(cudaMemsetAsync(e->tot.p, 0, sizeof(WaveTotals), s));
 
       TRY(e->launch("lookup_count", [&] {
-        lookup_count_kernel<<<(unsigned)((npos + kCountPerBlock - 1) / kCountPerBlock), kCountThreads, 0, s>>>(
-            w, e->pos_hits.p, e->tot.p);
+        const uint32_t ch = lookup_chunks(npos);
+        const uint64_t span = (uint64_t)ch * kCountPerBlock;
+        lookup_count_kernel<<<(unsigned)((npos + span - 1) / span), kCountThreads, 0, s>>>(w, ch, e->pos_hits.p,
+                                                                                          e->tot.p);
       }));
       TRY(e->launch(
           "np_scan",
@@ -1439,8 +1441,10 @@ int hz_generate_seeds(hz_engine *e, uint32_t slot, int rev, uint32_t start, uint
     w.occ_cap = e->cfg.occ_cap;
   w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
     TRY(e->launch("lookup_count", [&] {
-      lookup_count_kernel<<<(w.npos + kCountPerBlock - 1) / kCountPerBlock, kCountThreads, 0, e->st>>>(w, e->pos_hits.p,
-                                                                                                       e->tot.p);
+      const uint32_t ch = lookup_chunks(w.npos);
+      const uint64_t span = (uint64_t)ch * kCountPerBlock;
+      lookup_count_kernel<<<(unsigned)((w.npos + span - 1) / span), kCountThreads, 0, e->st>>>(w, ch, e->pos_hits.p,
+                                                                                              e->tot.p);
     }));
     CK(cudaMemcpyAsync(e->h_tot.p, e->tot.p, sizeof(WaveTotals), cudaMemcpyDeviceToHost, e->st));
     TRY(e->sync());

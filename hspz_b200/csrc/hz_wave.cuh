@@ -156,80 +156,97 @@ __device__ __forceinline__ uint32_t last_le(const unsigned long long *v, uint32_
 }
 
 // ---------------------------------------------------------------------------
-// Per flat position: total hits of its seeds.
+// Per flat position: total hits of its seeds.  A block walks `chunks`
+// consecutive chunks of kCountPerBlock positions (up to 16, fewer when the
+// wave is small, so that every SM still gets blocks), so the search for its
+// first call (log2(calls) dependent loads) is paid once per block and the
+// threads' calls only advance after it.
 constexpr int kCountThreads = 256;
 constexpr int kCountPerBlock = 1024;
+constexpr uint32_t kCountMaxChunks = 16;
 
-__global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, uint32_t *__restrict__ pos_hits,
+// Chunks per block for a wave of npos positions: as many as keep at least
+// ~600 blocks (four per SM) in the grid.
+inline uint32_t lookup_chunks(uint64_t npos) {
+  const uint64_t per = npos / (600ull * kCountPerBlock);
+  return (uint32_t)(per < 1 ? 1 : per > kCountMaxChunks ? kCountMaxChunks : per);
+}
+
+__global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, uint32_t chunks,
+                                                                     uint32_t *__restrict__ pos_hits,
                                                                      WaveTotals *__restrict__ tot) {
   __shared__ uint32_t s_c0;
-  uint32_t p0 = blockIdx.x * kCountPerBlock;
-  if (threadIdx.x == 0) s_c0 = call_of(w.calls, w.ncalls, p0);
+  const uint32_t base = blockIdx.x * chunks * kCountPerBlock;
+  if (threadIdx.x == 0) s_c0 = call_of(w.calls, w.ncalls, base);
   __syncthreads();
   uint32_t c = s_c0;
   uint32_t valid = 0;
   constexpr int kPer = kCountPerBlock / kCountThreads;
-  if (w.nbr_hits && w.per_pos > 1) {
-    // all of the thread's k-mers first, then their neighbourhood counts, so
-    // the count gathers of its positions are in flight together
-    uint32_t kmer[kPer];
-#pragma unroll
-    for (int i = 0; i < kPer; i++) {
-      const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
-      kmer[i] = kInvalidKmer;
-      if (p < w.npos) {
-        while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
-        uint32_t qpos;
-        position_seed(w, w.calls[c], p, &qpos, &kmer[i]);
-      }
-    }
-    uint32_t sum[kPer];
-#pragma unroll
-    for (int i = 0; i < kPer; i++) {
-      sum[i] = 0;
-      if (kmer[i] != kInvalidKmer) {
-        valid++;
-        sum[i] = __ldg(w.nbr_hits + kmer[i]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < kPer; i++) {
-      const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
-      if (p < w.npos) pos_hits[p] = sum[i];
-    }
-    for (int d = 16; d > 0; d >>= 1) valid += __shfl_down_sync(0xffffffffu, valid, d);
-    if ((threadIdx.x & 31) == 0 && valid) atomicAdd(&tot->valid, (unsigned long long)valid);
-    return;
-  }
+  const bool by_table = w.nbr_hits && w.per_pos > 1;
 #pragma unroll 1
-  for (int i = 0; i < kPer; i++) {
-    uint32_t p = p0 + i * kCountThreads + threadIdx.x;
-    if (p >= w.npos) break;
-    while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
-    CallDev cd = w.calls[c];
-    uint32_t qpos, kmer, sum = 0;
-    if (position_seed(w, cd, p, &qpos, &kmer)) {
-      valid++;
-      // every seed's bucket bounds are loaded before any is used, so the
-      // loads are in flight together
-      uint32_t hi[kMaxCare + 1], lo[kMaxCare + 1];
+  for (uint32_t chunk = 0; chunk < chunks; chunk++) {
+    const uint32_t p0 = base + chunk * kCountPerBlock;
+    if (p0 >= w.npos) break;
+    if (by_table) {
+      // all of the thread's k-mers first, then their neighbourhood counts, so
+      // the count gathers of its positions are in flight together
+      uint32_t kmer[kPer];
 #pragma unroll
-      for (uint32_t v = 0; v < kMaxCare + 1; v++) {
-        hi[v] = lo[v] = 0;
-        if (v < w.per_pos) {
-          const uint32_t k = seed_variant(kmer, v);
-          hi[v] = __ldg(w.index_table + k);
-          lo[v] = k ? __ldg(w.index_table + k - 1) : 0u;
+      for (int i = 0; i < kPer; i++) {
+        const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
+        kmer[i] = kInvalidKmer;
+        if (p < w.npos) {
+          while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+          uint32_t qpos;
+          position_seed(w, w.calls[c], p, &qpos, &kmer[i]);
+        }
+      }
+      uint32_t sum[kPer];
+#pragma unroll
+      for (int i = 0; i < kPer; i++) {
+        sum[i] = 0;
+        if (kmer[i] != kInvalidKmer) {
+          valid++;
+          sum[i] = __ldg(w.nbr_hits + kmer[i]);
         }
       }
 #pragma unroll
-      for (uint32_t v = 0; v < kMaxCare + 1; v++) {
-        uint32_t c = hi[v] - lo[v];
-        if (w.occ_cap && c > w.occ_cap) c = 0;  // find_num_hits with the occurrence cap
-        sum += c;
+      for (int i = 0; i < kPer; i++) {
+        const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
+        if (p < w.npos) pos_hits[p] = sum[i];
       }
+      continue;
     }
-    pos_hits[p] = sum;
+#pragma unroll 1
+    for (int i = 0; i < kPer; i++) {
+      uint32_t p = p0 + i * kCountThreads + threadIdx.x;
+      if (p >= w.npos) break;
+      while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+      CallDev cd = w.calls[c];
+      uint32_t qpos, kmer, sum = 0;
+      if (position_seed(w, cd, p, &qpos, &kmer)) {
+        valid++;
+        // every seed's bucket bounds are loaded before any is used, so the
+        // loads are in flight together
+        uint32_t hi[kMaxCare + 1], lo[kMaxCare + 1];
+#pragma unroll
+        for (uint32_t v = 0; v < kMaxCare + 1; v++) {
+          hi[v] = lo[v] = 0;
+          if (v < w.per_pos) {
+            const uint32_t k = seed_variant(kmer, v);
+            hi[v] = __ldg(w.index_table + k);
+            lo[v] = k ? __ldg(w.index_table + k - 1) : 0u;
+          }
+        }
+#pragma unroll
+        for (uint32_t v = 0; v < kMaxCare + 1; v++) {
+          uint32_t cnt = hi[v] - lo[v];
+          if (w.occ_cap && cnt > w.occ_cap) cnt = 0;  // find_num_hits with the occurrence cap
+          sum += cnt;
+        }
+      }
+      pos_hits[p] = sum;
+    }
   }
   for (int d = 16; d > 0; d >>= 1) valid += __shfl_down_sync(0xffffffffu, valid, d);
   if ((threadIdx.x & 31) == 0 && valid) atomicAdd(&tot->valid, (unsigned long long)valid);
