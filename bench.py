@@ -457,14 +457,18 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = peaks()
 
+    knobs = json.loads(args.tuning) if args.tuning else {}
+    cell_bytes = 2.0 if knobs.get("gate_version") == 1 else 0.75
+
     def summarize(r):
         ms, tot, prof, steps = r["ms"], r["tot"], r["prof"], r["steps"]
         per_s = steps * world / (ms / 1000)
         gate_ms, gate_n = prof.get("gate", (0.0, 0))
         # dominant kernel: the fused expansion + X-drop gate.  Algorithmic
-        # bytes: 2 B per scored cell (reference + query code) + 4 B per hit
-        # (its pos_table entry).
-        gate_bytes = (2.0 * tot["cells"] + 4.0 * tot["hits"]) * steps
+        # bytes: per scored cell the reference and query codes -- 0.75 B at
+        # 2 bits + 1 special bit per base (the lockstep gate), 2 B at 8-bit
+        # codes (the lane-refill gate) -- and 4 B per hit (its pos_table entry)
+        gate_bytes = (cell_bytes * tot["cells"] + 4.0 * tot["hits"]) * steps
         gate_gbs = gate_bytes / (gate_ms / 1000) / 1e9 if gate_ms else None
         lk_ms = prof.get("lookup_count", (0.0, 0))[0]
         # seed lookup per valid query position: its code byte, one 4-byte
@@ -636,7 +640,8 @@ def run_ours(args, rank, world, local_rank):
                          "frac": g["achieved"] / peak if g["achieved"] else None, "traffic": traffic,
                          "peak_kind": peak_kind, "spec_peak": 8000.0,
                          "frac_of_spec": g["achieved"] / 8000.0 if g["achieved"] else None,
-                         "note": "issue-bound integer kernel; algorithmic bytes = 2 B per scored cell + 4 B per hit"},
+                         "note": f"issue-bound integer kernel; algorithmic bytes = {cell_bytes:g} B per scored "
+                                 f"cell + 4 B per hit"},
             "lookup_roofline": dict(head["lookup"], kernel="lookup_count", peak=peak, unit="GB/s",
                                     note="9 B per valid query position: code byte, neighbourhood count, "
                                          "count written"),
