@@ -357,6 +357,7 @@ struct hz_engine {
   uint32_t gate_cap = 128;  // the autotuner's usual choice
   int gate_blocks_per_sm = 0;
   uint64_t wave_positions = 1ull << 27;  // seed positions per batched wave
+  uint64_t wave_hits_cap = 1ull << 33;    // hits per batched wave of several calls (tile table <= 512 MB)
   // CUDA graph of the batched wave chain
   bool use_graph = false;
   bool capturing = false;  // a wave chain is being captured on `st`
@@ -528,6 +529,10 @@ template <int TW> int launch_gate(hz_engine *e, const GateArgs &ga) {
   unsigned grid = (unsigned)(e->sm_count * per_sm);
   return e->launch("gate", [&] { gate_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(ga); });
 }
+
+// run_wave's answer for a wave of several calls that holds too many hits:
+// nothing was kept, and the caller reruns the calls in smaller waves.
+constexpr int kSplitWave = 1;
 
 // Runs calls[0..n) as one wave and appends its deduped HSPs, in call order
 // and LASTZ order within each MAX_HITS scope, to *out.  `seeds` (device) is
@@ -865,6 +870,10 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       return fail(HZ_E_INVALID, "the first seed of a call holds more than max_hits=%u hits; the reference's MAX_HITS "
                                 "walk has no valid cut there", e->max_hits);
     bool again = false;
+    // a wave of several calls holding more hits than wave_hits_cap is cut
+    // smaller (run_calls halves its position budget), so the grow-only wave
+    // buffers stay bounded on repeat-dense input
+    if (n > 1 && t.hits > e->wave_hits_cap) return kSplitWave;
     if (t.status & 4u) {  // the gate skipped the wave: its tile table was too small
       e->tile_cap = (uint32_t)std::min<uint64_t>(t.hits / (uint64_t)e->gate_tile + 1024, 0xFFFFFFF0ull);
       again = true;
@@ -1006,16 +1015,22 @@ int stage_ascii(hz_engine *e, const uint8_t *const *ascii, const uint64_t *lens,
 // Runs `calls` through batched waves of at most wave_positions positions.
 int run_calls(hz_engine *e, std::vector<HostCall> *calls, std::vector<WaveRecord> *recs, hz_stats *st) {
   size_t i = 0;
+  uint64_t budget = e->wave_positions;  // halved whenever a wave holds more than wave_hits_cap hits
   while (i < calls->size()) {
     size_t j = i;
     uint64_t npos = 0;
-    while (j < calls->size() && (j == i || npos + ((*calls)[j].end - (*calls)[j].start) <= e->wave_positions)) {
+    while (j < calls->size() && (j == i || npos + ((*calls)[j].end - (*calls)[j].start) <= budget)) {
       npos += (*calls)[j].end - (*calls)[j].start;
       j++;
     }
     size_t before = recs->size();
-    TRY(run_wave(e, calls->data() + i, j - i, nullptr, e->cfg.transitions, recs, st, e->device_dedup,
-                 e->use_graph));
+    const int rc = run_wave(e, calls->data() + i, j - i, nullptr, e->cfg.transitions, recs, st, e->device_dedup,
+                            e->use_graph);
+    if (rc == kSplitWave) {  // nothing of the wave was kept: run its calls in smaller waves
+      budget = std::max<uint64_t>(budget / 2, 1);
+      continue;
+    }
+    TRY(rc);
     for (size_t k = before; k < recs->size(); k++) (*recs)[k].call += (uint32_t)i;
     i = j;
   }
@@ -2032,6 +2047,9 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   } else if (k == "wave_positions") {
     if (value < 1 || value >= (1ll << 31)) return fail(HZ_E_INVALID, "wave_positions must be 1..2^31-1");
     e->wave_positions = (uint64_t)value;
+  } else if (k == "wave_hits_cap") {
+    if (value < (1ll << 20)) return fail(HZ_E_INVALID, "wave_hits_cap must be at least 2^20");
+    e->wave_hits_cap = (uint64_t)value;
   } else if (k == "plain_streams") {
     if (value < 1 || value > 4) return fail(HZ_E_INVALID, "plain_streams must be 1..4");
     e->plain_streams = (int)value;
@@ -2287,6 +2305,7 @@ void share_target(hz_engine *w, const hz_engine *e) {
   w->gate_cap = e->gate_cap;
   w->gate_blocks_per_sm = e->gate_blocks_per_sm;
   w->wave_positions = e->wave_positions;
+  w->wave_hits_cap = e->wave_hits_cap;
   w->device_dedup = e->device_dedup;
   w->device_dedup_min = e->device_dedup_min;
   w->use_graph = e->use_graph;

@@ -208,7 +208,7 @@ class Engine:
 
     def set_tuning(self, **knobs):
         """Launch-shape knobs: gate_version, gate_tile, gate_cap,
-        gate_blocks_per_sm, wave_positions, device_dedup, device_dedup_min,
+        gate_blocks_per_sm, wave_positions, wave_hits_cap, device_dedup, device_dedup_min,
         graph, plain_streams, tile_cap, cand_cap, raw_cap.  Results never
         depend on them."""
         for k, v in knobs.items():

@@ -231,7 +231,10 @@ int hz_engine_profile_reset(hz_engine *e);
  * "gate_tile" (hits per gate warp tile: 64, 128, 256),
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
- * "wave_positions" (seed positions per batched wave), "device_dedup" (1: the
+ * "wave_positions" (seed positions per batched wave), "wave_hits_cap" (a
+ * batched wave of several calls holding more seed hits than this, default
+ * 2^33, is run again as smaller waves, which bounds the hit-dependent wave
+ * buffers on repeat-dense input), "device_dedup" (1: the
  * batched form dedups on the device, and so does a plain-form call holding at
  * least "device_dedup_min" raw HSPs (default 65536); 0: every dedup on the
  * host, as the reference does),
