@@ -478,7 +478,8 @@ bool gate2_usable(const hz_engine *e) {
       const int32_t v = e->cfg.sub_mat[r * kNuc + q];
       if (v < -128 || v > 127) return false;
     }
-  return true;
+  // the group states a round keeps modulo 2^16 (gate2_kernel, near16)
+  return (int64_t)e->cfg.xdrop + kRound * 255 < 32768;
 }
 
 template <int TW> size_t gate2_smem() { return sizeof(Gate2Smem<TW>); }

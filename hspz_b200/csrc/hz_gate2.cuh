@@ -75,13 +75,15 @@ struct WarpTile2 {
   uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
   uint32_t hit_r[TW];     // reference anchor
   uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
-  int32_t grp[2 * kGroups][32];  // running sum and maximum of each lane at the start of each group of a round
+  // each lane's running sum (low half) and maximum (high half) at the start
+  // of each group of a round, both modulo 2^16 (near16 restores them)
+  uint32_t grp[kGroups][32];
 };
 
 template <int TW>
 struct Gate2Smem {
   int32_t sub[64];
-  int8_t tbl[4][256];  // score of the pair of codes a byte of a round's index word holds (see pair_words)
+  int8_t tbl[16];  // score of the pair of ACGT codes: reference code | query code << 2 (see pair_words)
   WarpTile2<TW> warp[kGateWarps];
 };
 
@@ -94,28 +96,35 @@ struct Gate2Args {
 };
 
 // The four index words of 16 cells: word j holds cells j, j+4, j+8, j+12 in
-// its bytes 0..3, each byte carrying that cell's reference code in bits
-// 2j..2j+1 and its query code in bits 2j+2..2j+3 (j < 3) or 0..1 (j = 3);
-// the other bits are other cells' codes, which tbl[j] ignores.
+// its bytes 0..3, each byte being that cell's table index (reference code |
+// query code << 2) with its upper four bits clear.  Every lane's score lookup
+// then falls in the same 16 bytes of shared memory, four banks, so a warp's
+// lookup is one wavefront whatever the codes.
 __device__ __forceinline__ void pair_words(uint32_t r, uint32_t q, uint32_t t[4]) {
-  const uint32_t q2 = q << 2, q6 = q >> 6;
-  t[0] = (r & 0x03030303u) | (q2 & ~0x03030303u);
-  t[1] = (r & 0x0C0C0C0Cu) | (q2 & ~0x0C0C0C0Cu);
-  t[2] = (r & 0x30303030u) | (q2 & ~0x30303030u);
-  t[3] = (r & 0xC0C0C0C0u) | (q6 & ~0xC0C0C0C0u);
-}
-
-__device__ __forceinline__ void pair_codes(int j, uint32_t b, uint32_t *r, uint32_t *q) {
-  *r = (b >> (2 * j)) & 3u;
-  *q = j < 3 ? (b >> (2 * j + 2)) & 3u : b & 3u;
+  const uint32_t x = (r & 0x33333333u) | ((q << 2) & 0xCCCCCCCCu);  // nibble n: index of cell 2n
+  const uint32_t y = ((r >> 2) & 0x33333333u) | (q & 0xCCCCCCCCu);  // nibble n: index of cell 2n + 1
+  t[0] = x & 0x0F0F0F0Fu;
+  t[1] = y & 0x0F0F0F0Fu;
+  t[2] = (x >> 4) & 0x0F0F0F0Fu;
+  t[3] = (y >> 4) & 0x0F0F0F0Fu;
 }
 
 // Score of cell k (0..15) of the 16 cells whose index words are t.
-__device__ __forceinline__ int32_t cell_score(const int8_t (*tbl)[256], const uint32_t t[4], int k) {
-  return tbl[k & 3][__byte_perm(t[k & 3], 0u, 0x4440u + (uint32_t)(k >> 2))];
+__device__ __forceinline__ int32_t cell_score(const int8_t *tbl, const uint32_t t[4], int k) {
+  return tbl[__byte_perm(t[k & 3], 0u, 0x4440u + (uint32_t)(k >> 2))];
 }
 
 __device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+
+// The value v with v = h (mod 2^16) and base - 32768 <= v < base + 32768.
+// A round's group states are read back against the running sum after all
+// its kRound cells, which lies within kRound * 128 of every stored sum; a
+// stored maximum read back exceeds its sum by at most xdrop plus one group's
+// fall, so every value read lies within kRound * 255 + xdrop of the base
+// (gate2_usable checks that this is below 32768).
+__device__ __forceinline__ int32_t near16(int32_t base, uint32_t h) {
+  return wadd(base, (int32_t)(int16_t)(uint16_t)(h - (uint32_t)base));
+}
 
 template <int TW>
 __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
@@ -125,14 +134,10 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
   Gate2Smem<TW> &sm = *reinterpret_cast<Gate2Smem<TW> *>(smem_raw);
   if (a.tot->status & 4u) return;  // no tile table: the host reruns the wave with a larger one
   if (threadIdx.x < 64) sm.sub[threadIdx.x] = a.sub[threadIdx.x];
-  for (uint32_t i = threadIdx.x; i < 1024; i += blockDim.x) {
-    uint32_t r, q;
-    pair_codes((int)(i >> 8), i & 255u, &r, &q);
-    sm.tbl[i >> 8][i & 255u] = (int8_t)a.sub[r * kNuc + q];
-  }
+  if (threadIdx.x < 16) sm.tbl[threadIdx.x] = (int8_t)a.sub[(threadIdx.x & 3u) * kNuc + (threadIdx.x >> 2)];
   __syncthreads();  // the block's only barrier
   WarpTile2<TW> &wt = sm.warp[threadIdx.x >> 5];
-  const int8_t(*tbl)[256] = sm.tbl;
+  const int8_t *tbl = sm.tbl;
   const uint32_t lane = threadIdx.x & 31;
   const int32_t X = a.xdrop;
   const uint32_t rlen = a.w.rlen, qtotal = a2.qtotal;
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
     // and before the first special base
     const uint32_t v = min(n, (uint32_t)kRound);
     const uint32_t sp0 = (RS0 | QS0) & (v >= 32 ? 0xFFFFFFFFu : ((1u << v) - 1u));
-    const uint32_t sp1 = (RS1 | QS1) & (v > 32 ? ((1u << (v - 32)) - 1u) : 0u);
+    const uint32_t sp1 = (RS1 | QS1) & (v >= 64 ? 0xFFFFFFFFu : v > 32 ? ((1u << (v - 32)) - 1u) : 0u);
     const uint32_t vv = sp0 ? (uint32_t)(__ffs(sp0) - 1) : sp1 ? 32u + (uint32_t)(__ffs(sp1) - 1) : v;
 
     // every lane scores all kRound cells; per eight-cell group it keeps the
@@ -314,8 +319,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
 #pragma unroll
       for (int gg = 0; gg < 2; gg++) {
         const int g = 2 * h + gg;
-        wt.grp[2 * g][lane] = S;
-        wt.grp[2 * g + 1][lane] = M;
+        wt.grp[g][lane] = __byte_perm((uint32_t)S, (uint32_t)M, 0x5410u);
         int32_t lo = 0x7FFFFFFF;
 #pragma unroll
         for (int i = 0; i < 8; i += 2) {
@@ -341,10 +345,16 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
       if (todo) {
         const uint32_t g = (uint32_t)(__ffs(todo) - 1);
         todo &= todo - 1;
-        int32_t Se = wt.grp[2 * g][lane], Me = wt.grp[2 * g + 1][lane];
+        const uint32_t st = wt.grp[g][lane];
+        int32_t Se = near16(S, st & 0xFFFFu), Me = near16(S, st >> 16);
         const uint32_t ch = g >> 1;  // the code word holding the group (constant indices keep Rc, Qc in registers)
-        const uint32_t hw = ch == 0 ? Rc[0] : ch == 1 ? Rc[1] : Rc[kChunks - 1];
-        const uint32_t qw = ch == 0 ? Qc[0] : ch == 1 ? Qc[1] : Qc[kChunks - 1];
+        uint32_t hw = Rc[0], qw = Qc[0];
+#pragma unroll
+        for (int k = 1; k < kChunks; k++)
+          if (ch == (uint32_t)k) {
+            hw = Rc[k];
+            qw = Qc[k];
+          }
         const uint32_t sh = (g & 1u) << 4;
         uint32_t tw[4];
         pair_words((hw >> sh) & 0xFFFFu, (qw >> sh) & 0xFFFFu, tw);
@@ -362,7 +372,7 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
           }
           if (dm) {
             ended = dropped = true;
-            res = g + 1 < (uint32_t)kGroups ? wt.grp[2 * g + 3][lane] : M;
+            res = g + 1 < (uint32_t)kGroups ? near16(S, wt.grp[g + 1][lane] >> 16) : M;
             used = 8 * g + (uint32_t)(__ffs(dm) - 1) + 1;
             todo = 0;
           }  // else the flag was loose: the next flagged group is looked at
