@@ -511,6 +511,42 @@ template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
   return e->launch("gate", [&] { gate2_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(a2); });
 }
 
+// The long candidates of a wave, extended to their ends in lockstep over the
+// packed sequences (long_kernel); runs only where the packed gate runs.
+int launch_long(hz_engine *e, const GateArgs &ga) {
+  static bool configured[64] = {false};
+  static std::mutex mu;
+  const size_t smem = sizeof(LongSmem);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!configured[e->device & 63]) {
+      CK(cudaFuncSetAttribute(long_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured[e->device & 63] = true;
+    }
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, long_kernel, kGateThreads, smem));
+  if (per_sm < 1) per_sm = 1;
+  LongArgs la;
+  la.ref = e->ref_p.half_ptr(0);
+  la.refr = e->ref_p.half_ptr(1);
+  la.qry = e->qry_p.half_ptr(0);
+  la.qryr = e->qry_p.half_ptr(1);
+  la.ref8 = ga.w.ref;
+  la.qry8 = ga.w.qbuf;
+  la.rlen = ga.w.rlen;
+  la.qtotal = (uint32_t)e->qstore.len;
+  la.calls = ga.w.calls;
+  la.cand = ga.cand;
+  la.cand_cap = ga.cand_cap;
+  la.tot = ga.tot;
+  memcpy(la.sub, ga.sub, sizeof(la.sub));
+  la.xdrop = ga.xdrop;
+  la.late_max_safe = ga.late_max_safe;
+  const unsigned grid = (unsigned)(e->sm_count * per_sm);
+  return e->launch("long", [&] { long_kernel<<<grid, kGateThreads, smem, e->st>>>(la); });
+}
+
 template <int TW> int launch_gate(hz_engine *e, const GateArgs &ga) {
   static bool configured[64] = {false};
   static std::mutex mu;  // serving workers launch from several host threads
@@ -819,6 +855,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
           case 256: TRY(launch_gate2<256>(e, ga)); break;
           default: TRY(launch_gate2<128>(e, ga)); break;
         }
+        TRY(launch_long(e, ga));
       } else {
         switch (e->gate_tile) {
           case 64: TRY(launch_gate<64>(e, ga)); break;

@@ -5,7 +5,8 @@
 //   np_*           scan of the counts; compaction of positions with hits
 //   scopes         per call: hit range and MAX_HITS dedup scopes
 //   gate           fused hit expansion + thread-per-hit X-drop score gate
-//   exact          warp-per-candidate X-drop with positions, entropy, accept
+//   long           lane-per-candidate exact extension of the gate's long candidates
+//   exact          warp-per-candidate X-drop positions, entropy, accept
 //
 // Semantics follow hspZ src/gpu/kernels.rs and src/gpu/mod.rs (cited per
 // kernel).  Hit indices are 64-bit across a wave (a call's own hit count is
@@ -60,7 +61,8 @@ struct WaveTotals {
   uint32_t status;  // bit 0: a call's first seed alone exceeds max_hits; bit 1: a call exceeds 2^32 hits
   uint32_t cand;    // gate candidates written (may exceed capacity)
   uint32_t raw;     // accepted HSPs written (may exceed capacity)
-  uint32_t pad[3];
+  uint32_t long_next;  // long_kernel's cursor over the candidates
+  uint32_t pad[2];
 };
 
 // Gate candidate: a hit whose score bound passes the threshold, or whose
@@ -69,9 +71,11 @@ struct Cand {
   uint32_t scope;  // dedup scope of the hit
   uint32_t r0;     // reference anchor
   uint32_t q0;     // query anchor, absolute in the query store
-  uint32_t call;   // call index | kLongFlag
-  int32_t rmax;    // the gate's right and left maxima (not for a long candidate)
+  uint32_t call;   // call index | kLongFlag | kDoneFlag
+  int32_t rmax;    // the right and left maxima: the gate's, or long_kernel's (kDoneFlag)
   int32_t lmax;
+  int32_t rpos;    // their positions, filled in by long_kernel only
+  int32_t lpos;
 };
 constexpr uint32_t kLongFlag = 1u << 31;
 
@@ -476,6 +480,7 @@ __global__ void __launch_bounds__(kScopeThreads) scopes_kernel(WaveIn w, const u
 
 #include "hz_gate.cuh"
 #include "hz_gate2.cuh"
+#include "hz_long.cuh"
 
 namespace hz {
 
@@ -656,13 +661,19 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(ExactArgs a) {
   const uint32_t warps = gridDim.x * (blockDim.x / 32);
   for (uint32_t i = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; i < ncand; i += warps) {
     Cand cd = a.cand[i];
-    bool is_long = cd.call & kLongFlag;
-    CallDev call = a.calls[cd.call & ~kLongFlag];
+    const bool done = (cd.call & kDoneFlag) != 0;  // long_kernel extended it: maxima and positions known
+    const bool is_long = !done && (cd.call & kLongFlag) != 0;
+    CallDev call = a.calls[cd.call & ~(kLongFlag | kDoneFlag)];
     const uint8_t *qry = a.qbuf + call.qoff;
     uint32_t q0 = cd.q0 - call.qoff, r0 = cd.r0;
     unsigned long long cells = 0;
     int32_t rmax, rpos, lmax, lpos;
-    if (is_long) {  // reached the gate's cap: long runs, four cells per lane
+    if (done) {
+      rmax = cd.rmax;
+      lmax = cd.lmax;
+      rpos = cd.rpos;
+      lpos = cd.lpos;
+    } else if (is_long) {  // reached the gate's cap: long runs, four cells per lane
       exact_dir4<false>(a.ref, qry, sub, a.xdrop, r0, q0, min(a.rlen - r0, call.qlen - q0), lane, &rmax, &rpos,
                         &cells);
       exact_dir4<true>(a.ref, qry, sub, a.xdrop, r0, q0, min(r0, q0), lane, &lmax, &lpos, &cells);
