@@ -334,6 +334,7 @@ struct hz_engine {
   // wave buffers
   DBuf<CallDev> calls;
   DBuf<uint32_t> pos_hits, np_pos, call_nz_lo, scope_call, raw_scope, tile_first, tile_call;
+  DBuf<uint32_t> pos_kmer, np_kmer;  // k-mer of every seed position, and of every position with hits
   uint32_t tile_cap = 1u << 23;  // entries of the gate's tile table (grows when a wave needs more)
   DBuf<unsigned long long> np_excl, call_hit_lo, scope_lo;
   DBuf<HitNz> np_partial, np_grand;
@@ -765,6 +766,8 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
   TRY(e->np_grand.ensure(1, s));
   TRY(e->np_excl.ensure(npos + 1, s));
   TRY(e->np_pos.ensure(npos + 1, s));
+  TRY(e->pos_kmer.ensure(npos, s));
+  TRY(e->np_kmer.ensure(npos + 1, s));
   TRY(e->call_hit_lo.ensure(n + 1, s));
   TRY(e->call_nz_lo.ensure(n + 1, s));
   TRY(e->tot.ensure(1, s));
@@ -787,6 +790,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
   w.nbr_hits = e->has_nbr ? e->nbr_hits.p : nullptr;
   const bool packed_q = e->qry_p.valid && e->shape.size <= 32 && e->qry_p.half >= e->qstore.len;
   w.qp2 = packed_q ? e->qry_p.half_ptr(0) : nullptr;
+  w.pos_kmer = e->pos_kmer.p;
 
   for (int attempt = 0; attempt < 8; attempt++) {  // each rerun fixes every capacity it found short
     uint32_t scope_cap = std::max<uint32_t>(e->scope_cap, (uint32_t)n * 2 + 16);
@@ -814,7 +818,8 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
             np_reduce_kernel<<<(unsigned)tiles, kScanThreads, 0, s>>>(e->pos_hits.p, npos, e->np_partial.p);
             scan_partials_kernel<HitNz><<<1, kScanThreads, 0, s>>>(e->np_partial.p, tiles, e->np_grand.p);
             np_emit_kernel<<<(unsigned)tiles, kScanThreads, 0, s>>>(e->pos_hits.p, npos, e->np_partial.p,
-                                                                    e->np_excl.p, e->np_pos.p);
+                                                                    e->np_excl.p, e->np_pos.p, e->pos_kmer.p,
+                                                                    e->np_kmer.p);
             np_totals_kernel<<<1, 32, 0, s>>>(e->np_grand.p, e->tot.p, e->np_excl.p);
           },
           4));
@@ -832,6 +837,7 @@ int run_wave(hz_engine *e, const HostCall *hc, size_t n, const uint64_t *seeds, 
       ga.w = w;
       ga.np_excl = e->np_excl.p;
       ga.np_pos = e->np_pos.p;
+      ga.np_kmer = e->np_kmer.p;
       ga.scope_lo = e->scope_lo.p;
       ga.scope_cap = scope_cap;
       ga.tot = e->tot.p;
@@ -1204,6 +1210,8 @@ void hz_engine_destroy(hz_engine *e) {
   e->calls.release();
   e->pos_hits.release();
   e->np_pos.release();
+  e->pos_kmer.release();
+  e->np_kmer.release();
   e->call_nz_lo.release();
   e->scope_call.release();
   e->raw_scope.release();
@@ -2267,6 +2275,7 @@ template <typename T> uint64_t dbytes(const DBuf<T> &b) { return b.p ? b.cap * s
 uint64_t wave_footprint(const hz_engine *w) {
   uint64_t b = w->aliases_query ? 0 : dbytes(w->qstore.buf) + dbytes(w->qry_p.blk);
   b += dbytes(w->qascii) + dbytes(w->calls) + dbytes(w->pos_hits) + dbytes(w->np_pos) + dbytes(w->call_nz_lo) +
+       dbytes(w->pos_kmer) + dbytes(w->np_kmer) +
        dbytes(w->scope_call) + dbytes(w->raw_scope) + dbytes(w->tile_first) + dbytes(w->tile_call) +
        dbytes(w->np_excl) + dbytes(w->call_hit_lo) + dbytes(w->scope_lo) + dbytes(w->np_partial) +
        dbytes(w->np_grand) + dbytes(w->tot) + dbytes(w->cand) + dbytes(w->raw) + dbytes(w->d_out);
@@ -2286,7 +2295,7 @@ void release_wave_buffers(hz_engine *w) {
   }
   w->qascii.release();
   for (DBuf<uint32_t> *x : {&w->pos_hits, &w->np_pos, &w->call_nz_lo, &w->scope_call, &w->raw_scope, &w->tile_first,
-                            &w->tile_call, &w->d_perm_a, &w->d_perm_b, &w->d_keys_a, &w->d_keys_b, &w->d_keep,
+                            &w->tile_call, &w->pos_kmer, &w->np_kmer, &w->d_perm_a, &w->d_perm_b, &w->d_keys_a, &w->d_keys_b, &w->d_keep,
                             &w->d_keep_excl, &w->d_hist, &w->d_hpart, &w->d_total})
     x->release();
   w->np_excl.release();
@@ -2302,16 +2311,16 @@ void release_wave_buffers(hz_engine *w) {
 }
 
 // Device working memory a request of `len` bases is expected to need while
-// it runs: both strands of the query store (1 B per base) and of the
-// per-position counts and compaction (16 B per position), plus the
-// hit-dependent buffers -- the gate's tile table (8 B per tile of hits),
-// candidates (16 B each), raw HSPs (20 B each) and their dedup scratch (24 B
-// each) -- at the server's current rates.
+// it runs: both strands of the query store (1 B per base, and 1 B for its
+// packed copy) and of the per-position counts, k-mers and compaction (24 B
+// per position), plus the hit-dependent buffers -- the gate's tile table (8 B
+// per tile of hits), candidates (32 B each), raw HSPs (20 B each) and their
+// dedup scratch (24 B each) -- at the server's current rates.
 uint64_t serve_estimate(const Server *s, uint64_t len) {
   const double pos = 2.0 * (double)len;
   const double hits = pos * s->hits_per_pos;
-  const double per_hit = 8.0 / s->gate_tile + 16.0 * s->cand_per_hit + 44.0 * s->raw_per_hit;
-  return (uint64_t)(pos * (1 + 16) + hits * per_hit) + (1ull << 20);
+  const double per_hit = 8.0 / s->gate_tile + 32.0 * s->cand_per_hit + 44.0 * s->raw_per_hit;
+  return (uint64_t)(pos * (2 + 24) + hits * per_hit) + (1ull << 20);
 }
 
 // Copies into `w` what a workspace shares with `e`: the resident target

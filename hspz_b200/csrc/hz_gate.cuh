@@ -70,6 +70,7 @@ struct GateArgs {
   WaveIn w;
   const unsigned long long *np_excl;
   const uint32_t *np_pos;
+  const uint32_t *np_kmer;  // k-mer of each position with hits (np_emit_kernel), or null
   const unsigned long long *scope_lo;
   uint32_t scope_cap;  // entries of scope_lo (a wave with more scopes is rerun)
   WaveTotals *tot;

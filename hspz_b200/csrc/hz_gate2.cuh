@@ -75,6 +75,7 @@ struct WarpTile2 {
   uint32_t hit_slot[TW];  // first hit of the hit's slot + 1 (mark, then max-scan)
   uint32_t hit_r[TW];     // reference anchor
   uint32_t hit_n[TW];     // cells to the right edge | cells to the left edge << 16 (each saturated)
+  uint32_t hdr[4];        // the claimed next tile's first position, the position after it, its call
   // each lane's running sum (low half) and maximum (high half) at the start
   // of each group of a round, both modulo 2^16 (near16 restores them)
   uint32_t grp[kGroups][32];
@@ -126,8 +127,18 @@ __device__ __forceinline__ int32_t near16(int32_t base, uint32_t h) {
   return wadd(base, (int32_t)(int16_t)(uint16_t)(h - (uint32_t)base));
 }
 
+// 4-byte global -> shared copy that completes asynchronously (no register
+// holds the value), and the wait for all of the thread's copies.
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <int TW>
-__global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
+__global__ void __launch_bounds__(kGateThreads, 4) gate2_kernel(Gate2Args a2) {
   static_assert(TW % 32 == 0, "a warp tile is a multiple of 32 hits");
   const GateArgs &a = a2.g;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -154,6 +165,11 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
   // current tile is handed out so that its latency is hidden (lane 0 holds it)
   bool claimed = false;
   unsigned long long claim = 0;
+  // The tile setup spreads a tile's (position, seed) pairs over the lanes:
+  // 32 / per_pos positions per pass, lane l on seed l % per_pos of position
+  // l / per_pos, so all bucket bounds of a pass are loaded at once.
+  const uint32_t per = w.per_pos, ppi = 32u / per, lpi = lane / per, lvar = lane - lpi * per;
+  bool hdr = false;  // the claimed tile's header is on its way into wt.hdr
   // Takes the next tile from the work queue and sets it up: the hits'
   // anchors, edge distances and slots (query anchor, call).  Every lane takes
   // part; lanes busy with an earlier tile's hits hold what they need of them
@@ -162,7 +178,9 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
     unsigned long long j = claim;
     if (!claimed && lane == 0) j = atomicAdd(&a.tot->tiles, 1ull);
     j = __shfl_sync(0xffffffffu, j, 0);
+    const bool have_hdr = claimed && hdr;
     claimed = false;
+    hdr = false;
     h0 = j * (unsigned long long)TW;
     cursor = 0;
     if (h0 >= total) {
@@ -171,40 +189,68 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
       return;
     }
     nt = (uint32_t)min((unsigned long long)TW, total - h0);
-    const uint32_t k0 = a.tile_first[j], k1 = a.tile_first[j + 1];
-    const uint32_t e1 = (k1 >= nz || a.np_excl[k1] == h0 + nt) ? k1 - 1 : k1;
-    uint32_t c = a.tile_call[j];
+    uint32_t k0, k1, c0;
+    if (have_hdr) {
+      cp_async_wait_all();
+      __syncwarp();
+      k0 = wt.hdr[0];
+      k1 = wt.hdr[1];
+      c0 = wt.hdr[2];
+    } else {
+      k0 = a.tile_first[j];
+      k1 = a.tile_first[j + 1];
+      c0 = a.tile_call[j];
+    }
+    // positions k0 .. kend cover the tile (k1, the next tile's first
+    // position, only if its hits start inside this one; the overlap test
+    // below sorts that out)
+    const uint32_t kend = min(k1, nz - 1);
+    const CallDev call0 = w.calls[c0];
+    const uint32_t next_off = c0 + 1 < w.ncalls ? w.calls[c0 + 1].pos_off : 0xFFFFFFFFu;
     __syncwarp();  // every lane has read what it needs of the previous tile
     for (uint32_t i = lane; i < nt; i += 32) wt.hit_slot[i] = 0;
     __syncwarp();
-    for (uint32_t k = k0 + lane; k <= e1; k += 32) {
-      uint32_t p = a.np_pos[k];
-      while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
-      CallDev cd = w.calls[c];
-      uint32_t qpos, kmer;
-      position_seed(w, cd, p, &qpos, &kmer);
-      unsigned long long lo = a.np_excl[k];
-      const uint32_t q_anchor = cd.qoff + qpos + w.shape.size;
-      for (uint32_t v0 = 0; v0 < w.per_pos; v0 += kLookupBatch) {
-        uint32_t beg[kLookupBatch], cnt[kLookupBatch];
-#pragma unroll
-        for (uint32_t u = 0; u < kLookupBatch; u++) {
-          cnt[u] = 0;
-          beg[u] = 0;
-          if (v0 + u < w.per_pos) cnt[u] = bucket(w, seed_variant(kmer, v0 + u), &beg[u]);
+    for (uint32_t kb = k0; kb <= kend; kb += ppi) {
+      const uint32_t k = kb + lpi;
+      const bool act = lpi < ppi && k <= kend;
+      uint32_t cnt = 0, beg = 0, qa = 0, c = c0;
+      unsigned long long lo = 0;
+      if (act) {
+        const uint32_t p = a.np_pos[k];
+        lo = a.np_excl[k];
+        uint32_t kmer, qpos;
+        CallDev cd = call0;
+        if (p >= next_off) {  // the tile reaches into a later call
+          while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+          cd = w.calls[c];
         }
+        if (a.np_kmer && !w.seeds) {
+          kmer = a.np_kmer[k];
+          qpos = cd.start + (p - cd.pos_off);
+        } else {
+          position_seed(w, cd, p, &qpos, &kmer);
+        }
+        qa = cd.qoff + qpos + w.shape.size;
+        cnt = bucket(w, seed_variant(kmer, lvar), &beg);
+      }
+      // the position's earlier seeds' hits come first: inclusive scan of the
+      // counts over the position's lanes
+      uint32_t incl = cnt;
 #pragma unroll
-        for (uint32_t u = 0; u < kLookupBatch; u++) {
-          unsigned long long hi = lo + cnt[u];
-          if (cnt[u] && hi > h0 && lo < h0 + nt) {
-            unsigned long long first = lo > h0 ? lo : h0;
-            uint32_t s = (uint32_t)(first - h0);
-            wt.slot_bst[s] = beg[u] + (uint32_t)(first - lo);
-            wt.slot_q[s] = q_anchor;
-            wt.slot_call[s] = c;
-            wt.hit_slot[s] = s + 1;
-          }
-          lo = hi;
+      for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t up = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lvar >= d) incl += up;
+      }
+      if (cnt) {
+        lo += incl - cnt;
+        const unsigned long long hi = lo + cnt;
+        if (hi > h0 && lo < h0 + nt) {
+          const unsigned long long first = lo > h0 ? lo : h0;
+          const uint32_t sl = (uint32_t)(first - h0);
+          wt.slot_bst[sl] = beg + (uint32_t)(first - lo);
+          wt.slot_q[sl] = qa;
+          wt.slot_call[sl] = c;
+          wt.hit_slot[sl] = sl + 1;
         }
       }
     }
@@ -271,6 +317,14 @@ __global__ void __launch_bounds__(kGateThreads) gate2_kernel(Gate2Args a2) {
     if (!claimed && !tiles_done && 2 * cursor >= nt) {
       if (lane == 0) claim = atomicAdd(&a.tot->tiles, 1ull);
       claimed = true;
+    } else if (claimed && !hdr) {
+      // a round after the claim: the claimed tile's header, copied into
+      // shared memory while this round is scored
+      const unsigned long long jn = __shfl_sync(0xffffffffu, claim, 0);
+      if (jn * (unsigned long long)TW < total && lane < 3)
+        cp_async4(&wt.hdr[lane], lane == 0 ? a.tile_first + jn : lane == 1 ? a.tile_first + jn + 1 : a.tile_call + jn);
+      cp_async_commit();
+      hdr = true;
     }
     unsigned need = __ballot_sync(0xffffffffu, !have);
     if (need && cursor >= nt && !tiles_done) next_tile();

@@ -48,6 +48,7 @@ struct WaveIn {
   // the query store packed 2 bits per base (forward half of pack2_kernel's
   // records), or null to read the 8-bit codes
   const uint4 *qp2;
+  uint32_t *pos_kmer;  // per flat position: its k-mer, written by lookup_count (or null)
 };
 
 // Device-side counters of a wave.
@@ -217,7 +218,10 @@ __global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, u
 #pragma unroll
       for (int i = 0; i < kPer; i++) {
         const uint32_t p = p0 + i * kCountThreads + threadIdx.x;
-        if (p < w.npos) pos_hits[p] = sum[i];
+        if (p < w.npos) {
+          pos_hits[p] = sum[i];
+          if (w.pos_kmer) w.pos_kmer[p] = kmer[i];
+        }
       }
       continue;
     }
@@ -250,6 +254,7 @@ __global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, u
         }
       }
       pos_hits[p] = sum;
+      if (w.pos_kmer) w.pos_kmer[p] = kmer;
     }
   }
   for (int d = 16; d > 0; d >>= 1) valid += __shfl_down_sync(0xffffffffu, valid, d);
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, u
 
 // Scan of (hits, has-hits) over positions, then compaction of the positions
 // with hits: np_excl = hits of the wave before the position, np_pos = its
-// flat index.
+// flat index, np_kmer = its k-mer (when lookup_count kept the k-mers).
 __global__ void __launch_bounds__(kScanThreads) np_reduce_kernel(const uint32_t *__restrict__ pos_hits, uint64_t n,
                                                                  HitNz *__restrict__ partial) {
   uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
@@ -278,7 +283,9 @@ __global__ void __launch_bounds__(kScanThreads) np_reduce_kernel(const uint32_t 
 __global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *__restrict__ pos_hits, uint64_t n,
                                                                const HitNz *__restrict__ partial,
                                                                unsigned long long *__restrict__ np_excl,
-                                                               uint32_t *__restrict__ np_pos) {
+                                                               uint32_t *__restrict__ np_pos,
+                                                               const uint32_t *__restrict__ pos_kmer,
+                                                               uint32_t *__restrict__ np_kmer) {
   uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
   HitNz acc = HitNz{0ull, 0u};
@@ -298,6 +305,7 @@ __global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *_
     if (v[i]) {
       np_excl[ex.n] = ex.h;
       np_pos[ex.n] = (uint32_t)(base + i);
+      if (np_kmer) np_kmer[ex.n] = pos_kmer[base + i];
       ex.h += v[i];
       ex.n += 1;
     }
