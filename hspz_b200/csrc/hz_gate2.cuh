@@ -279,15 +279,34 @@ __global__ void __launch_bounds__(kGateThreads, 4) gate2_kernel(Gate2Args a2) {
         }
     }
     __syncwarp();
-    for (uint32_t i = lane; i < nt; i += 32) {
-      uint32_t s = wt.hit_slot[i] - 1;
-      uint32_t r0 = __ldg(w.pos_table + wt.slot_bst[s] + (i - s)) + w.shape.size;
-      uint32_t q0 = wt.slot_q[s];
-      const CallDev &cd = w.calls[wt.slot_call[s]];
-      uint32_t nr = min(w.rlen - r0, cd.qoff + cd.qlen - q0);
-      uint32_t nl = min(r0, q0 - cd.qoff);
-      wt.hit_r[i] = r0;
-      wt.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
+    {  // each hit's reference anchor and edge distances; a lane's TW / 32
+       // pos_table words and calls are loaded before any is used
+      constexpr int PER = TW / 32;
+      uint32_t r0[PER], q0[PER], qb[PER], qe[PER];
+#pragma unroll
+      for (int u = 0; u < PER; u++) {
+        const uint32_t i = lane + 32u * (uint32_t)u;
+        r0[u] = 0;
+        q0[u] = qb[u] = qe[u] = 0;
+        if (i < nt) {
+          const uint32_t s = wt.hit_slot[i] - 1;
+          r0[u] = __ldg(w.pos_table + wt.slot_bst[s] + (i - s));
+          q0[u] = wt.slot_q[s];
+          const CallDev &cd = w.calls[wt.slot_call[s]];
+          qb[u] = cd.qoff;
+          qe[u] = cd.qoff + cd.qlen;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < PER; u++) {
+        const uint32_t i = lane + 32u * (uint32_t)u;
+        if (i < nt) {
+          const uint32_t r = r0[u] + w.shape.size;
+          const uint32_t nr = min(w.rlen - r, qe[u] - q0[u]), nl = min(r, q0[u] - qb[u]);
+          wt.hit_r[i] = r;
+          wt.hit_n[i] = min(nr, 0xFFFFu) | (min(nl, 0xFFFFu) << 16);
+        }
+      }
     }
     __syncwarp();
   };
