@@ -471,11 +471,13 @@ def run_ours(args, rank, world, local_rank):
         gate_bytes = (cell_bytes * tot["cells"] + 4.0 * tot["hits"]) * steps
         gate_gbs = gate_bytes / (gate_ms / 1000) / 1e9 if gate_ms else None
         lk_ms = prof.get("lookup_count", (0.0, 0))[0]
-        # seed lookup per valid query position: its code byte, one 4-byte
-        # neighbourhood hit count (the per-k-mer table built with the target
-        # holds the capped hits of all 13 seeds) and the 4-byte count written
+        # seed lookup per valid query position: its base at 2 bits + 1 special
+        # bit, one 4-byte neighbourhood hit count (the per-k-mer table built
+        # with the target holds the capped hits of all 13 seeds), and the
+        # count and the k-mer written (4 B each; the gate's tile setup reads
+        # the k-mer back)
         positions = tot["seeds"] / 13.0
-        lk_bytes = positions * 9.0 * steps
+        lk_bytes = positions * 12.375 * steps
         lk_gbs = lk_bytes / (lk_ms / 1000) / 1e9 if lk_ms else None
         return {"hits_per_s": tot["hits"] * per_s, "extended_bp_per_s": tot["cells"] * per_s,
                 "ms_per_step": ms / steps, "steps": steps, "warmup": r["warmup"],
@@ -643,8 +645,8 @@ def run_ours(args, rank, world, local_rank):
                          "note": f"issue-bound integer kernel; algorithmic bytes = {cell_bytes:g} B per scored "
                                  f"cell + 4 B per hit"},
             "lookup_roofline": dict(head["lookup"], kernel="lookup_count", peak=peak, unit="GB/s",
-                                    note="9 B per valid query position: code byte, neighbourhood count, "
-                                         "count written"),
+                                    note="12.375 B per valid query position: packed base (0.375 B), "
+                                         "neighbourhood count, count and k-mer written"),
             "forms": summ,
             "batched_over_plain": (summ["batched"]["hits_per_s"] / summ["plain"]["hits_per_s"]
                                    if len(summ) == 2 else None),

@@ -17,6 +17,11 @@ struct ShapeDev {
   uint32_t size;
   uint32_t kmer_size;
   uint32_t pos[kMaxCare];
+  // the care positions as runs of consecutive bases, in care order
+  uint32_t nruns;
+  uint32_t is_12of19;  // the pattern is 12of19's (TTT0T00TT00T0T0TTTT): kmer_12of19 applies
+  uint32_t run_start[kMaxCare];
+  uint32_t run_len[kMaxCare];
 };
 
 // Everything the extension needs besides sequence and anchors.

@@ -164,6 +164,17 @@ int parse_shape(const char *spec, ShapeDev *sh) {
     return fail(HZ_E_INVALID, "seed %s has %u care positions; the seed table requires 4..=15", spec, k);
   sh->size = n;
   sh->kmer_size = k;
+  static const uint32_t k12of19[12] = {0, 1, 2, 4, 7, 8, 11, 13, 15, 16, 17, 18};
+  sh->is_12of19 = n == 19 && k == 12 && !memcmp(sh->pos, k12of19, sizeof(k12of19));
+  for (uint32_t t = 0; t < k; t++) {
+    if (t && sh->pos[t] == sh->pos[t - 1] + 1) {
+      sh->run_len[sh->nruns - 1]++;
+    } else {
+      sh->run_start[sh->nruns] = sh->pos[t];
+      sh->run_len[sh->nruns] = 1;
+      sh->nruns++;
+    }
+  }
   return HZ_OK;
 }
 

@@ -130,6 +130,37 @@ __device__ __forceinline__ uint32_t kmer_packed(const uint4 *__restrict__ blk, u
   return kmer;
 }
 
+// The k-mer of the window that starts j bases into 32 packed bases w64 (base
+// i at bits 2i..2i+1), for patterns of at most 32 - j bases: the care digits
+// come out a run of consecutive care positions at a time, first care
+// position in the lowest bits, and one digit reversal puts it on top.
+__device__ __forceinline__ uint32_t kmer_runs(uint64_t w64, uint32_t j, const ShapeDev &sh) {
+  const uint64_t x = w64 >> (2 * j);
+  uint32_t le = 0, at = 0;
+  for (uint32_t r = 0; r < sh.nruns; r++) {
+    const uint32_t len2 = 2 * sh.run_len[r];
+    le |= ((uint32_t)(x >> (2 * sh.run_start[r])) & ((1u << len2) - 1u)) << at;
+    at += len2;
+  }
+  uint32_t rv = __brev(le);
+  rv = ((rv >> 1) & 0x55555555u) | ((rv & 0x55555555u) << 1);
+  return rv >> (32 - 2 * sh.kmer_size);
+}
+
+// kmer_runs for the 12of19 pattern (TTT0T00TT00T0T0TTTT: runs of 3, 1, 2,
+// 1, 1 and 4 care positions at bases 0, 4, 7, 11, 13 and 15) with constant
+// shifts: each run's field moves to its place in one shift and one mask.
+// lo, hi: 32 packed bases; j <= 13.
+__device__ __forceinline__ uint32_t kmer_12of19(uint32_t lo, uint32_t hi, uint32_t j) {
+  const uint32_t xlo = __funnelshift_r(lo, hi, 2 * j), xhi = hi >> (2 * j);
+  const uint32_t y = __funnelshift_r(xlo, xhi, 14);  // bases 7.. of the window
+  const uint32_t le = (xlo & 0x3Fu) | ((xlo >> 2) & (0x3u << 6)) | ((xlo >> 6) & (0xFu << 8)) |
+                      ((xlo >> 10) & (0x3u << 12)) | ((xlo >> 12) & (0x3u << 14)) | (y & (0xFFu << 16));
+  uint32_t rv = __brev(le);
+  rv = ((rv >> 1) & 0x55555555u) | ((rv & 0x55555555u) << 1);
+  return rv >> 8;
+}
+
 // ---------------------------------------------------------------------------
 // Seed table on device (SeedTable::build, src/seed.rs:135-180): k-mers of
 // the strided reference positions, compaction of the valid ones in position

@@ -165,7 +165,10 @@ __device__ __forceinline__ uint32_t last_le(const unsigned long long *v, uint32_
 // consecutive chunks of kCountPerBlock positions (up to 16, fewer when the
 // wave is small, so that every SM still gets blocks), so the search for its
 // first call (log2(calls) dependent loads) is paid once per block and the
-// threads' calls only advance after it.
+// threads' calls only advance after it.  With the neighbourhood table and
+// the packed query, a thread takes four consecutive positions of a chunk:
+// one 32-base window gives their four k-mers, their four counts are
+// gathered together, and counts and k-mers go out as 16-byte stores.
 constexpr int kCountThreads = 256;
 constexpr int kCountPerBlock = 1024;
 constexpr uint32_t kCountMaxChunks = 16;
@@ -187,11 +190,69 @@ __global__ void __launch_bounds__(kCountThreads) lookup_count_kernel(WaveIn w, u
   uint32_t c = s_c0;
   uint32_t valid = 0;
   constexpr int kPer = kCountPerBlock / kCountThreads;
+  static_assert(kPer % 4 == 0, "a thread's counts go out as 16-byte stores");
   const bool by_table = w.nbr_hits && w.per_pos > 1;
+  // kPer consecutive positions per thread from one 32-base packed window
+  const bool by_window = by_table && w.qp2 && !w.seeds && w.shape.size + kPer - 1 <= 32;
+  const uint32_t win_mask = w.shape.size >= 32 ? 0xFFFFFFFFu : (1u << w.shape.size) - 1u;
 #pragma unroll 1
   for (uint32_t chunk = 0; chunk < chunks; chunk++) {
     const uint32_t p0 = base + chunk * kCountPerBlock;
     if (p0 >= w.npos) break;
+    if (by_window) {
+      const uint32_t p = p0 + kPer * threadIdx.x;
+      if (p >= w.npos) continue;
+      while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+      const CallDev cd = w.calls[c];
+      const uint32_t next_off = c + 1 < w.ncalls ? w.calls[c + 1].pos_off : 0xFFFFFFFFu;
+      uint32_t kmer[kPer], sum[kPer];
+      if (p + kPer - 1 < next_off && p + kPer - 1 < w.npos) {  // positions of one call: one window
+        uint32_t lo, hi, sp;
+        window32(w.qp2, cd.qoff + cd.start + (p - cd.pos_off), &lo, &hi, &sp);
+        const uint64_t w64 = (uint64_t)hi << 32 | lo;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++)
+          kmer[j] = ((sp >> j) & win_mask) ? kInvalidKmer
+                    : w.shape.is_12of19          ? kmer_12of19(lo, hi, j)
+                                                 : kmer_runs(w64, j, w.shape);
+      } else {  // a call boundary or the wave's end among them
+        uint32_t cc = c;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) {
+          kmer[j] = kInvalidKmer;
+          if (p + j < w.npos) {
+            while (cc + 1 < w.ncalls && w.calls[cc + 1].pos_off <= p + j) cc++;
+            uint32_t qpos;
+            position_seed(w, w.calls[cc], p + j, &qpos, &kmer[j]);
+          }
+        }
+      }
+#pragma unroll
+      for (uint32_t j = 0; j < kPer; j++) {
+        sum[j] = 0;
+        if (kmer[j] != kInvalidKmer) {
+          valid++;
+          sum[j] = __ldg(w.nbr_hits + kmer[j]);
+        }
+      }
+      if (p + kPer - 1 < w.npos) {
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j += 4) {
+          *reinterpret_cast<uint4 *>(pos_hits + p + j) = make_uint4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+          if (w.pos_kmer)
+            *reinterpret_cast<uint4 *>(w.pos_kmer + p + j) =
+                make_uint4(kmer[j], kmer[j + 1], kmer[j + 2], kmer[j + 3]);
+        }
+      } else {
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++)
+          if (p + j < w.npos) {
+            pos_hits[p + j] = sum[j];
+            if (w.pos_kmer) w.pos_kmer[p + j] = kmer[j];
+          }
+      }
+      continue;
+    }
     if (by_table) {
       // all of the thread's k-mers first, then their neighbourhood counts, so
       // the count gathers of its positions are in flight together
