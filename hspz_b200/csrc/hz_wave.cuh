@@ -356,6 +356,10 @@ __global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *_
     acc.h += v[i];
     acc.n += v[i] > 0;
   }
+  // the k-mers of the positions with hits, loaded while the block scans
+  uint32_t km[kScanItems];
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) km[i] = np_kmer && v[i] ? pos_kmer[base + i] : 0u;
   HitNz tot;
   HitNz ex = block_exclusive_scan<HitNz>(acc, &tot);
   HitNz off = partial[blockIdx.x];
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(kScanThreads) np_emit_kernel(const uint32_t *_
     if (v[i]) {
       np_excl[ex.n] = ex.h;
       np_pos[ex.n] = (uint32_t)(base + i);
-      if (np_kmer) np_kmer[ex.n] = pos_kmer[base + i];
+      if (np_kmer) np_kmer[ex.n] = km[i];
       ex.h += v[i];
       ex.n += 1;
     }
