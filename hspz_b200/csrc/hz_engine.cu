@@ -365,6 +365,10 @@ struct hz_engine {
   uint32_t cand_cap = 1u << 20, raw_cap = 1u << 20, scope_cap = 0;
   // tuning
   int gate_version = 2;  // 2: lockstep gate over packed sequences (when the scores allow), 1: lane-refill gate
+  // hz_run_batched's records, kept between calls so that repeated passes
+  // reuse the host memory instead of growing (and faulting in) a new vector
+  std::vector<WaveRecord> batch_recs;
+  int gate_sparse = -1;  // lockstep gate tile setup: -1 chosen from the target's buckets, 0 pairs, 1 lane per position
   int gate_tile = 128;  // hits per gate warp tile
   uint32_t gate_cap = 128;  // the autotuner's usual choice
   int gate_blocks_per_sm = 0;
@@ -496,20 +500,20 @@ bool gate2_usable(const hz_engine *e) {
 
 template <int TW> size_t gate2_smem() { return sizeof(Gate2Smem<TW>); }
 
-template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
+template <int TW, bool SPARSE> int launch_gate2_as(hz_engine *e, const GateArgs &ga) {
   static bool configured[64] = {false};
   static std::mutex mu;  // serving workers launch from several host threads
   size_t smem = gate2_smem<TW>();
   {
     std::lock_guard<std::mutex> lock(mu);
     if (!configured[e->device & 63]) {
-      CK(cudaFuncSetAttribute(gate2_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CK(cudaFuncSetAttribute(gate2_kernel<TW, SPARSE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       configured[e->device & 63] = true;
     }
   }
   int per_sm = e->gate_blocks_per_sm;
   if (per_sm <= 0) {
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate2_kernel<TW>, kGateThreads, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate2_kernel<TW, SPARSE>, kGateThreads, smem));
     if (per_sm < 1) per_sm = 1;
   }
   Gate2Args a2;
@@ -520,7 +524,19 @@ template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
   a2.qryr = e->qry_p.half_ptr(1);
   a2.qtotal = (uint32_t)e->qstore.len;
   unsigned grid = (unsigned)(e->sm_count * per_sm);
-  return e->launch("gate", [&] { gate2_kernel<TW><<<grid, kGateThreads, smem, e->st>>>(a2); });
+  return e->launch("gate", [&] { gate2_kernel<TW, SPARSE><<<grid, kGateThreads, smem, e->st>>>(a2); });
+}
+
+// The sparse tile setup when a tile is expected to span more than three
+// passes of (position, seed) pairs (32 / per_pos positions each), from the
+// hits per query position: seeds per position times the average bucket.
+template <int TW> int launch_gate2(hz_engine *e, const GateArgs &ga) {
+  const double per_bucket = (double)e->n_pos / (double)(1ull << (2 * e->shape.kmer_size));
+  const double hits_per_pos = std::max(ga.w.per_pos * per_bucket, 1e-9);
+  const double positions_per_pass = (double)(32 / ga.w.per_pos);
+  const bool sparse =
+      e->gate_sparse >= 0 ? e->gate_sparse == 1 : (double)TW / hits_per_pos > 3.0 * positions_per_pass;
+  return sparse ? launch_gate2_as<TW, true>(e, ga) : launch_gate2_as<TW, false>(e, ga);
 }
 
 // The long candidates of a wave, extended to their ends in lockstep over the
@@ -1105,13 +1121,44 @@ int check_range(hz_engine *e, uint32_t start, uint32_t end) {
   return HZ_OK;
 }
 
+// f(begin, end) over [0, n) on up to 16 host threads (one for small n, or
+// if a thread cannot be started): output copies of hundreds of millions of
+// records are bound by first-touch page faults, which threads take in
+// parallel.
+template <typename F> void parallel_ranges(size_t n, F f) {
+  const size_t kMinPerThread = 1u << 20;
+  unsigned t = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 16u);
+  t = (unsigned)std::min<size_t>(t, n / kMinPerThread);
+  if (t <= 1) {
+    f((size_t)0, n);
+    return;
+  }
+  const size_t per = (n + t - 1) / t;
+  std::vector<std::thread> th;
+  size_t done = 0;  // ranges below `done` have a thread
+  try {
+    for (unsigned i = 0; i < t; i++) {
+      const size_t a = i * per, b = std::min(n, a + per);
+      if (a >= b) break;
+      th.emplace_back(f, a, b);
+      done = b;
+    }
+  } catch (...) {
+  }
+  if (done < n) f(done, n);
+  for (auto &x : th) x.join();
+}
+
 int copy_out_segments(const std::vector<WaveRecord> &recs, hz_segment_pair **out, uint64_t *n) {
   *out = nullptr;
   *n = recs.size();
   if (recs.empty()) return HZ_OK;
   *out = (hz_segment_pair *)malloc(recs.size() * sizeof(hz_segment_pair));
   if (!*out) return fail(HZ_E_OOM, "host allocation");
-  for (size_t i = 0; i < recs.size(); i++) (*out)[i] = recs[i].h;
+  hz_segment_pair *o = *out;
+  parallel_ranges(recs.size(), [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; i++) o[i] = recs[i].h;
+  });
   return HZ_OK;
 }
 
@@ -1765,15 +1812,19 @@ int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *s
   hz_stats local;
   memset(&local, 0, sizeof local);
   std::vector<HostCall> calls;
-  std::vector<WaveRecord> recs;
+  std::vector<WaveRecord> &recs = e->batch_recs;
+  recs.clear();
   TRY(run_all_staged(e, &calls, &recs, &local));
   if (!recs.empty()) {
     *out = (hz_batch_record *)malloc(recs.size() * sizeof(hz_batch_record));
     if (!*out) return fail(HZ_E_OOM, "host allocation");
-    for (size_t k = 0; k < recs.size(); k++) {
-      const HostCall &c = calls[recs[k].call];
-      (*out)[k] = hz_batch_record{c.query, c.interval, c.strand, recs[k].h};
-    }
+    hz_batch_record *o = *out;
+    parallel_ranges(recs.size(), [&](size_t a, size_t b) {
+      for (size_t k = a; k < b; k++) {
+        const HostCall &c = calls[recs[k].call];
+        o[k] = hz_batch_record{c.query, c.interval, c.strand, recs[k].h};
+      }
+    });
   }
   *n = recs.size();
   if (stats) *stats = local;
@@ -2088,6 +2139,9 @@ int hz_engine_set_tuning(hz_engine *e, const char *key, int64_t value) {
   } else if (k == "gate_version") {
     if (value != 1 && value != 2) return fail(HZ_E_INVALID, "gate_version must be 1 or 2");
     e->gate_version = (int)value;
+  } else if (k == "gate_sparse") {
+    if (value < -1 || value > 1) return fail(HZ_E_INVALID, "gate_sparse must be -1, 0 or 1");
+    e->gate_sparse = (int)value;
   } else if (k == "gate_cap") {
     if (value < 8 || value > 65528 || value % 8) return fail(HZ_E_INVALID, "gate_cap must be a multiple of 8 in 8..65528");
     e->gate_cap = (uint32_t)value;
@@ -2359,6 +2413,7 @@ void share_target(hz_engine *w, const hz_engine *e) {
   w->has_target = true;
   w->owns_target = false;
   w->gate_version = e->gate_version;
+  w->gate_sparse = e->gate_sparse;
   w->gate_tile = e->gate_tile;
   w->gate_cap = e->gate_cap;
   w->gate_blocks_per_sm = e->gate_blocks_per_sm;

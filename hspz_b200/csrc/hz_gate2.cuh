@@ -137,7 +137,11 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <int TW>
+// SPARSE: the setup for targets whose buckets hold few positions, where a
+// 128-hit tile spans many query positions (10-20 Mbp bins): a lane per
+// position instead of per (position, seed) pair.  The engine picks it from
+// the target's average bucket size.
+template <int TW, bool SPARSE>
 __global__ void __launch_bounds__(kGateThreads, 4) gate2_kernel(Gate2Args a2) {
   static_assert(TW % 32 == 0, "a warp tile is a multiple of 32 hits");
   const GateArgs &a = a2.g;
@@ -210,6 +214,50 @@ __global__ void __launch_bounds__(kGateThreads, 4) gate2_kernel(Gate2Args a2) {
     __syncwarp();  // every lane has read what it needs of the previous tile
     for (uint32_t i = lane; i < nt; i += 32) wt.hit_slot[i] = 0;
     __syncwarp();
+    if constexpr (SPARSE) {
+      // a lane per position, its seeds' bucket bounds loaded five at a time
+      // (more would spill in this register budget)
+      for (uint32_t k = k0 + lane; k <= kend; k += 32) {
+        const uint32_t p = a.np_pos[k];
+        unsigned long long lo = a.np_excl[k];
+        uint32_t kmer, qpos, c = c0;
+        CallDev cd = call0;
+        if (p >= next_off) {  // the tile reaches into a later call
+          while (c + 1 < w.ncalls && w.calls[c + 1].pos_off <= p) c++;
+          cd = w.calls[c];
+        }
+        if (a.np_kmer && !w.seeds) {
+          kmer = a.np_kmer[k];
+          qpos = cd.start + (p - cd.pos_off);
+        } else {
+          position_seed(w, cd, p, &qpos, &kmer);
+        }
+        const uint32_t qa = cd.qoff + qpos + w.shape.size;
+        constexpr uint32_t kBatch = 5;
+        for (uint32_t v0 = 0; v0 < per; v0 += kBatch) {
+          uint32_t beg[kBatch], cnt[kBatch];
+#pragma unroll
+          for (uint32_t u = 0; u < kBatch; u++) {
+            cnt[u] = 0;
+            beg[u] = 0;
+            if (v0 + u < per) cnt[u] = bucket(w, seed_variant(kmer, v0 + u), &beg[u]);
+          }
+#pragma unroll
+          for (uint32_t u = 0; u < kBatch; u++) {
+            const unsigned long long hi = lo + cnt[u];
+            if (cnt[u] && hi > h0 && lo < h0 + nt) {
+              const unsigned long long first = lo > h0 ? lo : h0;
+              const uint32_t sl = (uint32_t)(first - h0);
+              wt.slot_bst[sl] = beg[u] + (uint32_t)(first - lo);
+              wt.slot_q[sl] = qa;
+              wt.slot_call[sl] = c;
+              wt.hit_slot[sl] = sl + 1;
+            }
+            lo = hi;
+          }
+        }
+      }
+    } else
     for (uint32_t kb = k0; kb <= kend; kb += ppi) {
       const uint32_t k = kb + lpi;
       const bool act = lpi < ppi && k <= kend;

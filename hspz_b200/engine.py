@@ -207,7 +207,7 @@ class Engine:
         N.check(N.lib().hz_engine_set_stream(self._h, C.c_void_p(stream_handle or None)))
 
     def set_tuning(self, **knobs):
-        """Launch-shape knobs: gate_version, gate_tile, gate_cap,
+        """Launch-shape knobs: gate_version, gate_sparse, gate_tile, gate_cap,
         gate_blocks_per_sm, wave_positions, wave_hits_cap, device_dedup, device_dedup_min,
         graph, plain_streams, tile_cap, cand_cap, raw_cap.  Results never
         depend on them."""

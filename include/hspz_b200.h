@@ -160,7 +160,9 @@ int hz_select_query(hz_engine *e, uint32_t index);
  * persistent gate launch over a device work queue, one read-back per wave)
  * instead of one launch chain per call.  Records are grouped by query, then
  * exactly as hz_run_pass orders them; each query's records equal what
- * hz_run_pass returns for that query alone. */
+ * hz_run_pass returns for that query alone.  The engine keeps the host
+ * buffer it assembles the records in (20 bytes per record) until it is
+ * destroyed, so a repeated pass does not allocate it again. */
 int hz_run_batched(hz_engine *e, hz_batch_record **out, uint64_t *n, hz_stats *stats);
 
 /* One line of a .segments file (hsp::Record, src/hsp.rs:179-187): the
@@ -228,6 +230,9 @@ int hz_engine_profile_reset(hz_engine *e);
  * them): "gate_version" (2, the default: the lockstep gate over 2-bit packed
  * sequences, used whenever every ACGT score fits a signed byte; 1: the
  * lane-refill gate over 8-bit codes, which also serves wider scores),
+ * "gate_sparse" (the lockstep gate's tile setup: -1, the default, chosen
+ * from the target's average bucket; 0 a lane per (position, seed) pair;
+ * 1 a lane per position, for targets whose tiles span many positions),
  * "gate_tile" (hits per gate warp tile: 64, 128, 256),
  * "gate_cap" (cells per direction before a hit goes to the warp kernel,
  * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),

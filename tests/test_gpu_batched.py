@@ -62,6 +62,7 @@ def test_batched_equals_plain_per_query(workload):
                                     dict(device_dedup=0, wave_positions=5_000), dict(graph=1),
                                     dict(graph=1, wave_positions=20_000, gate_tile=64),
                                     dict(gate_version=1), dict(gate_version=1, gate_tile=64, gate_cap=8),
+                                    dict(gate_sparse=0), dict(gate_sparse=1), dict(gate_sparse=0, gate_cap=8),
                                     dict(wave_hits_cap=1 << 20)])
 def test_launch_shapes_do_not_change_results(workload, tuning):
     target, chunks = workload

@@ -74,16 +74,19 @@ def test_repeat_dense_batched_equals_plain(pair):
     assert st["hits"] == hits
 
 
+@pytest.mark.parametrize("gate_version", [2, 1])
 @pytest.mark.parametrize("gate_cap", [8, 64])
-def test_long_extensions_through_the_warp_kernel(pair, gate_cap):
-    """A small gate cap sends most hits to the warp kernel as long
-    extensions (four cells per lane there); records and counts still equal
+def test_long_extensions(pair, gate_cap, gate_version):
+    """A small gate cap sends most hits on as long candidates: with the
+    lockstep gate to the lane-per-candidate long kernel (maxima and their
+    first positions from its 48-cell rounds), with the lane-refill gate to
+    the warp kernel (four cells per lane).  Records and counts still equal
     the oracle's."""
     t, q = pair
     sm = EngineConfig().sub_mat
     want, st_o = oracle_run(t, q, sm, occ_cap=1000)
     with Engine(EngineConfig(occ_cap=1000)) as e:
-        e.set_tuning(gate_cap=gate_cap)
+        e.set_tuning(gate_cap=gate_cap, gate_version=gate_version)
         e.load_target(t)
         e.swap_query_ascii(q)
         got, st = e.run_pass()
