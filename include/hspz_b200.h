@@ -234,8 +234,10 @@ int hz_engine_profile_reset(hz_engine *e);
  * from the target's average bucket; 0 a lane per (position, seed) pair;
  * 1 a lane per position, for targets whose tiles span many positions),
  * "gate_tile" (hits per gate warp tile: 64, 128, 256),
- * "gate_cap" (cells per direction before a hit goes to the warp kernel,
- * multiple of 8, 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
+ * "gate_cap" (cells per direction before a hit leaves the gate as a long
+ * candidate -- for the lane-per-candidate long kernel after the lockstep
+ * gate, for the warp kernel after the lane-refill gate -- multiple of 8,
+ * 8..65528), "gate_blocks_per_sm" (0 = occupancy maximum),
  * "wave_positions" (seed positions per batched wave), "wave_hits_cap" (a
  * batched wave of several calls holding more seed hits than this, default
  * 2^33, is run again as smaller waves, which bounds the hit-dependent wave
